@@ -1,0 +1,166 @@
+"""The accuracy-report rows that read this path's reductions (accusim/accuracy.py:19-221) and the dt
+calibration loop (accusim/advisor.py:58-79): energy drift, momentum drift, angular momentum,
+mass and charge ledgers, and the Richardson dt / dt/2 / dt/4 timestep error. Thresholds and
+formulas are the reference's."""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .units import si
+
+PASS, WARN, FAIL, NA = "PASS", "WARN", "FAIL", "n/a"
+
+
+@dataclass
+class Check:
+    name: str
+    status: str
+    value: float | None
+    detail: str
+
+    def row(self):
+        v = "" if self.value is None else f"{self.value:.2e}"
+        return f"  [{self.status:>4}] {self.name:<22} {v:>10}  {self.detail}"
+
+
+def _grade(x, good, ok):
+    return PASS if x <= good else WARN if x <= ok else FAIL
+
+
+def energy_drift(tr) -> float:
+    """max|E - E0| / max(|E0|, max|KE|, max|PE|) (accusim/accuracy.py:70-76)."""
+    E = tr.total_energy
+    scale = max(abs(E[0]), np.max(np.abs(tr.kinetic)), np.max(np.abs(tr.potential)), 1e-300)
+    return float(np.max(np.abs(E - E[0])) / scale)
+
+
+def momentum_drift(tr, s) -> float:
+    """max|P - P0| / sum m|v| (accusim/accuracy.py:86-91)."""
+    P = np.array(tr.momentum)
+    pscale = max(float(np.sum(s.masses[:, None] * np.abs(s.vel))), 1e-300)
+    return float(np.max(np.linalg.norm(P - P[0], axis=1)) / pscale)
+
+
+class AccuracyReport:
+    def __init__(self, checks):
+        self.checks = checks
+
+    def __getitem__(self, name) -> Check:
+        for c in self.checks:
+            if c.name == name:
+                return c
+        raise KeyError(name)
+
+    @property
+    def ok(self) -> bool:
+        return all(c.status != FAIL for c in self.checks)
+
+    def __str__(self):
+        nf = sum(c.status == FAIL for c in self.checks)
+        nw = sum(c.status == WARN for c in self.checks)
+        if nf:
+            head = f"Accuracy report (PROBLEMS FOUND: {nf} failed, {nw} warnings)"
+        elif nw:
+            head = f"Accuracy report (no failures, {nw} warning{'s' * (nw != 1)})"
+        else:
+            head = "Accuracy report (all applicable checks passed)"
+        return "\n".join([head] + [c.row() for c in self.checks])
+
+    @classmethod
+    def build(cls, sim, convergence_duration=None):
+        tr, s = sim.trajectory, sim.system
+        if len(tr.t) < 2:
+            raise ValueError("run the simulation before asking for a report")
+        checks = [Check("units", PASS, None, "every input was dimension-checked on entry")]
+        integ = sim.integrator
+        conservative = all(f.conservative for f in sim.forces) and not integ.thermostat
+        external = any(f.external for f in sim.forces)
+        walls = s.box is not None and not s.periodic
+        central = all(f.central for f in sim.forces)
+        if conservative:
+            d = energy_drift(tr)
+            checks.append(Check("energy", _grade(d, 1e-5, 1e-3), d,
+                                "max |E(t)-E0| / energy scale (incl. reaction ledger)"))
+        else:
+            checks.append(Check("energy", NA, None, "not conserved by design"))
+        if not external and not walls and not integ.thermostat:
+            dp = momentum_drift(tr, s)
+            checks.append(Check("momentum", _grade(dp, 1e-9, 1e-6), dp, "max |P(t)-P0| / sum m|v|"))
+        else:
+            checks.append(Check("momentum", NA, None, "external field, walls or thermostat"))
+        if central and not external and s.box is None and not integ.thermostat and s.dim in (2, 3):
+            Lm = np.array(tr.angular_momentum)
+            lscale = max(float(np.sum(np.linalg.norm(np.cross(s.pos, s.masses[:, None] * s.vel), axis=-1)))
+                         if s.dim == 3 else float(np.sum(np.abs(np.cross(s.pos, s.masses[:, None] * s.vel)))), 1e-300)
+            dl = float(np.max(np.linalg.norm(Lm - Lm[0], axis=1)) / lscale)
+            checks.append(Check("angular momentum", _grade(dl, 1e-9, 1e-6), dl, "max |L(t)-L0| / sum |r x p|"))
+        else:
+            checks.append(Check("angular momentum", NA, None, "needs central forces in open space"))
+        M = np.array(tr.mass)
+        dm = float(np.max(np.abs(M - M[0])) / M[0]) if M[0] else 0.0
+        checks.append(Check("mass-energy", _grade(dm, 1e-12, 1e-9), dm, "rest mass + released/c^2"))
+        Qc = np.array(tr.charge)
+        qscale = max(float(np.sum(np.abs(s.charges))), 1e-300)
+        dq = float(np.max(np.abs(Qc - Qc[0])) / qscale)
+        checks.append(Check("charge", _grade(dq, 1e-12, 1e-9), dq, "total charge"))
+        if convergence_duration is not None:
+            checks.append(timestep_convergence(sim, convergence_duration))
+        return cls(checks)
+
+
+def richardson_check(finals, n, order) -> Check:
+    """Observed order and Richardson estimate from finals at dt, dt/2, dt/4 (accusim/accuracy.py:207-221)."""
+    size = max(float(np.ptp(finals[2])), 1e-300)
+    roundoff = 1e-13 * np.sqrt(n * 4)
+    e1 = float(np.sqrt(np.mean((finals[0] - finals[1]) ** 2))) / size
+    e2 = float(np.sqrt(np.mean((finals[1] - finals[2]) ** 2))) / size
+    if e1 < 10 * roundoff:
+        return Check("timestep error", PASS, e1, "converged to floating-point round-off")
+    p = np.log2(e1 / e2)
+    est = e1 * 2 ** p / (2 ** p - 1) if p > 0.2 else e1
+    if p < 0.5 * order:
+        return Check("timestep error", FAIL if est > 1e-2 else WARN, est,
+                     f"observed order {p:.1f} (expected {order}): chaotic or dt too large; trust statistics, "
+                     "not trajectories")
+    return Check("timestep error", _grade(est, 1e-6, 1e-3), est,
+                 f"est. position error at dt (relative to system size), observed order {p:.1f}/{order}")
+
+
+def timestep_convergence(sim, duration, start=None) -> Check:
+    """Re-run from the initial state at dt, dt/2, dt/4 and estimate the error at dt
+    (accusim/accuracy.py:191-221)."""
+    if sim.integrator.stochastic or sim.reactions:
+        return Check("timestep error", NA, None, "stochastic run: compare ensemble statistics instead")
+    base = start or sim._initial
+    T = si(duration, "s")
+    n = max(int(round(T / sim.dt)), 1)
+    finals = []
+    for k in (1, 2, 4):
+        c = base.clone(dt=sim.dt / k)
+        c.run(steps=n * k, record_every=10 ** 9, positions=False)
+        finals.append(c.system.pos.copy())
+    return richardson_check(finals, n, sim.integrator.order)
+
+
+def calibrate_dt(sim, trial_duration, energy_tol=1e-6, max_halvings=12):
+    """Halve dt until a trial run conserves energy to `energy_tol`; sets and returns (sim.dt, drift)
+    (accusim/advisor.py:58-79)."""
+    if sim.integrator.stochastic or sim.integrator.thermostat or not all(f.conservative for f in sim.forces):
+        raise ValueError("calibrate_dt needs conservative, deterministic physics")
+    if sim.dt is None:
+        raise ValueError("set sim.dt to the largest dt to try")
+    T = si(trial_duration, "s")
+    dt = sim.dt
+    drift = float("nan")
+    for _ in range(max_halvings + 1):
+        trial = sim.clone(dt=dt)
+        n = max(int(round(T / dt)), 1)
+        tr = trial.run(steps=n, record_every=max(1, n // 200), positions=False)
+        drift = energy_drift(tr)
+        if drift <= energy_tol:
+            sim.dt = dt
+            return dt, drift
+        dt /= 2
+    raise RuntimeError(f"energy drift {drift:.2e} still above {energy_tol:.0e} after {max_halvings} halvings")
