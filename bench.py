@@ -1,0 +1,393 @@
+"""Benchmark: LJ/DSF atom-steps/s on one B200 at stated energy drift vs the FP64 path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lj1m|nacl4096|argon864] [--impl ours|reference]
+
+Default workload: 1,048,576-atom LJ fluid (fcc 64^3, rho* 0.8442, T* 0.72, rc 2.5 sigma, skin 0.3 sigma,
+dt* 0.005), FP32-compensated pair forces with FP64 integration, the step loop as CUDA graphs. A step is
+one VelocityVerlet step of the whole system (forces, both kicks, drift, skin test, list rebuilds when due).
+Inputs (positions, velocities, 400+ MB of neighbour lists) exceed the 126 MB L2, so no flush is needed.
+Under torchrun each rank advances its own independent system (replicas only; no collective in the step
+loop) and rank 0 prints one JSON line. `--impl reference` times the CPU restatement of the reference
+NumPy path on this host's cores (all of them, one process each) for the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LJ/DSF atom-steps/s on 1 B200 at stated energy drift vs FP64 oracle"
+UNIT = "atom-steps/s"
+BYTES_PER_ATOM_STEP = 128        # FP64 x, v read+write (96 B) + FP32 image write+read (32 B)
+FLOP_PER_PAIR = {"lj": 40, "dsf": 70}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(name, seed=0):
+    from devinproj_b200 import configs
+    cfg = workload_meta(name)
+    if name == "lj1m":
+        s, forces, dt = configs.lj_large(64, seed=seed)
+    elif name == "nacl4096":
+        s, forces, dt = configs.nacl4096(seed=seed)
+    else:
+        s, forces, dt = configs.argon864(seed=seed)
+    return s, forces, dt, cfg
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
+
+
+def cpu_baseline_port(steps_budget_s=15.0):
+    """The oracle (NumPy restatement of the reference path) on a 32,000-atom sample of the same fluid, 1 core."""
+    import numpy as np
+
+    from devinproj_b200 import configs
+    from oracle import accusim_port as port
+    s, lj = configs.lj_fluid(20, seed=0)
+    st = port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                    [("Ar", configs.AR_MASS, 0.0)])
+    run = port.Run(st, [port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)],
+                   0.005 * configs.AR_TAU)
+    run.run(1)
+    t0 = time.perf_counter()
+    run.run(1)
+    t1 = time.perf_counter() - t0
+    m = int(max(3, min(60, steps_budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    run.run(m)
+    dt = time.perf_counter() - t0
+    return {"value": s.n * m / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle NumPy FP64 port, 32000-atom fcc 20^3 at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, "
+                      f"{m} steps after 2 warm-up steps, 1 process"}
+
+
+def _ref_worker(args):
+    nc, steps, warmup, seed = args
+    import numpy as np  # noqa: F401
+
+    from devinproj_b200 import configs
+    from oracle import accusim_port as port
+    s, _ = configs.lj_fluid(nc, seed=seed)
+    st = port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                    [("Ar", configs.AR_MASS, 0.0)])
+    run = port.Run(st, [port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)],
+                   0.005 * configs.AR_TAU)
+    run.run(max(warmup, 1), record_every=10 ** 9)
+    t0 = time.perf_counter()
+    run.run(steps, record_every=10 ** 9)
+    return s.n * steps, time.perf_counter() - t0
+
+
+def reference_arm(args, cfg):
+    """The reference's CPU path (the oracle port: the reference is Python and cannot travel) on all host
+    cores: one process per core, each an independent bounded sample of the workload."""
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    per_atom_step_s = 11e-6   # measured NumPy cell-list cost per atom-step on this class of host
+    budget = 150.0
+    n_target = budget / max(args.steps + args.warmup, 1) / per_atom_step_s
+    nc = int(max(4, min(20, math.floor((n_target / 4) ** (1 / 3)))))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(nc, args.steps, args.warmup, 100 + k) for k in range(cores)])
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    span = max(r[1] for r in res)
+    value = work / span
+    sample = (f"oracle NumPy FP64 port of the reference path, {cores} processes x fcc {nc}^3 "
+              f"({4 * nc ** 3} atoms) at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, {args.steps} timed steps "
+              f"after {args.warmup} warm-up (wall {wall:.0f} s)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * span / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--workload", default="lj1m")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--record-every", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args, full_config(workload_meta(args.workload), args, world))
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from devinproj_b200 import _lib
+    from devinproj_b200.engine import ACC, LEN, VEL, start_engine
+
+    s, forces, dt, cfg = workload(args.workload, seed=rank)
+    eng, rlist, hs = start_engine([s], forces, [dt], rec_cap=max(args.steps // args.record_every + 2, 4))
+    n = s.n
+    pairs_lj, pairs_dsf = eng.count_pairs()
+    step_blocks, coop_blocks, slots = eng.launch_info()
+    init = eng.records(1)[0, 0].copy()
+    stream = torch.cuda.current_stream()
+
+    # warm-up (also instantiates the timed graph's sibling shapes)
+    eng.run(args.warmup, 0, True)
+    torch.cuda.synchronize()
+    eng.check("warm-up")
+    rb0 = eng.status().rebuilds
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------------------------------------------------------- timed region (device events)
+    eng.run(args.steps, args.record_every, True)   # instantiate the graph outside the timed region
+    torch.cuda.synchronize()
+    eng.check("graph warm-up")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.25)
+        barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(stream)
+        eng.run(args.steps, args.record_every, True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        wall = time.perf_counter() - w0
+    ms = e0.elapsed_time(e1)
+    st = eng.check("timed run")
+    nrec = args.steps // args.record_every + (1 if args.steps % args.record_every else 0)
+    recs = eng.records(nrec)[:, 0, :]
+    rebuilds_timed = st.rebuilds - rb0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * args.steps * world / (ms / 1e3)
+
+    # energy / momentum over the timed run (the report's metrics), in engine units
+    E = recs[:, 0] + recs[:, 1]
+    scale = max(abs(E[0]), np.max(np.abs(recs[:, 0])), np.max(np.abs(recs[:, 1])))
+    drift = float(np.max(np.abs(E - E[0])) / scale)
+    slope = float(np.polyfit(np.arange(len(E)) * args.record_every, E, 1)[0]) if len(E) > 2 else 0.0
+    pos_d, vel_d, acc_d = eng.get_state()
+    masses = np.array([x.mass for x in s.species])[s.sp]
+    pscale = float(np.sum(masses[:, None] * np.abs(vel_d.cpu().numpy() * VEL)))
+    P = recs[:, 2:5] * (1.66053906660e-27 * VEL)
+    mom_drift = float(np.max(np.linalg.norm(P - P[0], axis=1)) / pscale)
+
+    # ---------------------------------------------------------------- per-kernel timing (eager, events)
+    k_step_ms, k_reb_ms, _ = eng.run_timed(min(args.steps, 1000), args.record_every)
+    torch.cuda.synchronize()
+    eng.check("timed eager run")
+
+    # ---------------------------------------------------------------- accuracy vs the FP64 path
+    # FP64 forces on the final state by the drop-in kernels (pinned to the reference to 1e-12)
+    s.pos = pos_d.cpu().numpy() * LEN
+    s.vel = vel_d.cpu().numpy() * VEL
+    F32 = acc_d.cpu().numpy() * ACC * masses[:, None]
+    F64 = np.zeros_like(F32)
+    U64 = 0.0
+    for f in forces:
+        Fi, Ui = f.compute(s)
+        F64 += Fi
+        U64 += Ui
+    f_err = float(np.sqrt(np.mean(np.sum((F32 - F64) ** 2, 1)) / np.mean(np.sum(F64 ** 2, 1))))
+
+    # ---------------------------------------------------------------- end to end (host buffers)
+    pos_h = (pos_d.cpu() * 1.0).pin_memory()
+    vel_h = vel_d.cpu().pin_memory()
+    out_p = torch.empty_like(pos_h).pin_memory()
+    out_v = torch.empty_like(vel_h).pin_memory()
+    dev_p = torch.empty_like(pos_d)
+    dev_v = torch.empty_like(vel_d)
+    eng.run(1, 0, True)
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        dev_p.copy_(pos_h, non_blocking=True)
+        dev_v.copy_(vel_h, non_blocking=True)
+        eng.load_state(dev_p, dev_v)
+        eng.run(1, 0, True)
+        p, v, _ = eng.get_state()
+        out_p.copy_(p, non_blocking=True)
+        out_v.copy_(v, non_blocking=True)
+        rec = eng.records(1)           # the step's energies: synchronises
+        pos_h, out_p = out_p, pos_h
+        vel_h, out_v = out_v, vel_h
+    torch.cuda.synchronize()
+    barrier()
+    e2e_s = time.perf_counter() - w0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = n * args.e2e_steps * world / e2e_s
+    eng.check("e2e")
+
+    peaks, peak_kind = measured_peaks()
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = clocks["sm_mhz"] or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or 1965.0
+    fp32_peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+    alg_bytes = BYTES_PER_ATOM_STEP * n
+    achieved_gbs = alg_bytes / (k_step_ms / 1e3) / 1e9
+    flops = FLOP_PER_PAIR["lj"] * pairs_lj + FLOP_PER_PAIR["dsf"] * pairs_dsf
+    achieved_tf = flops / (k_step_ms / 1e3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(cfg["workload"])
+        except ValueError:
+            traffic = None
+    launches = 2 + 2 * args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32-pairs/f64-state", "data": "synthetic (seeded fcc lattice, MB velocities)",
+        "config": full_config(cfg, args, world),
+        "accuracy": {"force_rms_rel_err_vs_fp64": f_err, "energy_drift_report_metric": drift,
+                     "energy_drift_per_step_rel": slope / scale if scale else 0.0,
+                     "momentum_drift_report_metric": mom_drift, "steps_in_drift_window": args.steps,
+                     "rebuilds_in_timed_region": int(rebuilds_timed)},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": traffic, "kernel": "k_step",
+                     "kernel_ms": k_step_ms, "list_kernel_ms": k_reb_ms, "peak_source": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "fp32": {"achieved_tflops": achieved_tf, "peak_tflops": fp32_peak,
+                              "frac": achieved_tf / fp32_peak, "pairs_lj": pairs_lj, "pairs_dsf": pairs_dsf,
+                              "peak_basis": f"{sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (sampled median)"}},
+        "clocks": clocks,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n + 64,
+                "steps": args.e2e_steps, "path": "pinned host pos/vel -> acs_engine_load_state -> 1 step graph -> "
+                                                  "acs_engine_get_state -> pinned host + energy record"},
+        "gpu_launches": launches,
+        "wall_s_timed": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+WORKLOADS = {
+    "lj1m": {"workload": "lj_fcc64_1048576", "atoms": 1048576, "rho_star": 0.8442, "T_star": 0.72,
+             "cutoff_sigma": 2.5, "skin_sigma": 0.3, "dt_star": 0.005, "forces": "LennardJones"},
+    "nacl4096": {"workload": "nacl_rocksalt16_4096", "atoms": 4096, "density_g_cm3": 1.55, "T_K": 1200,
+                 "dsf_alpha_per_A": 0.2, "dsf_rc_A": 12.0, "dt_fs": 1.0, "forces": "LennardJones+DampedShiftedCoulomb"},
+    "argon864": {"workload": "argon_fcc6_864", "atoms": 864, "box_sigma": 10.229, "T_K": 94.4, "dt_fs": 10.0,
+                 "forces": "LennardJones"},
+}
+
+
+def workload_meta(name):
+    """Workload description without building device state (for the reference arm)."""
+    if name not in WORKLOADS:
+        raise SystemExit(f"unknown workload {name}")
+    return dict(WORKLOADS[name])
+
+
+def full_config(cfg, args, world):
+    return dict(cfg, l2="inputs larger than L2" if cfg["atoms"] >= 1 << 20 else "inputs resident in L2 (small system)",
+                record_every=args.record_every,
+                parallelism=f"independent replicas x{world}" if world > 1 else "single system")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1219 @@
+// Device-resident MD engine: FP32-compensated pair forces with FP64 integration, for one system or a
+// batch of independent replicas advanced together, captured in CUDA graphs.
+//
+// Per step the graph runs two kernels:
+//   k_step    one thread per atom slot: Kahan-compensated FP32 LJ / DSF pair sum over the atom's full
+//             neighbour list -> FP64 acceleration -> second half-kick (step completed; records taken
+//             here) -> first half-kick of the next step -> drift -> FP32 image for the next step ->
+//             displacement test that flags its replica for a list rebuild. (accusim/integrators.py:25-31
+//             with the two kicks of consecutive steps fused.)
+//   k_rebuild cooperative, bounded grid barriers; returns at once unless a replica is flagged (or
+//             records are due): re-bins flagged replicas into cells of size >= list radius, reorders
+//             their atoms by cell, rebuilds the lists with the reference's FP64 pair filter
+//             (accusim/forces.py:279-321, :86-98), and reduces per-replica records.
+//
+// Positions are held as FP64 offsets u from the origin of the cell the atom was binned into at the last
+// rebuild (continuous between rebuilds); the absolute wrapped position is py_mod(origin + u, box), as
+// accusim/system.py:124-129 keeps it. Pair displacements are d = (img_j - img_i) + m * cell, with the FP32
+// images img = float(u) and the integer image shift m in {-1,0,1}^3 stored with the neighbour index.
+// d_ji == -d_ij bitwise, so pair forces are exactly antisymmetric.
+#include <cooperative_groups.h>
+#include <math.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "accusim_b200_engine.h"
+#include "common.cuh"
+
+using namespace acs;
+
+namespace {
+
+constexpr int kMaxRep = 8192;   // replicas per engine (flag bitmap in shared memory)
+constexpr int kRecW = 8;        // KE, PE, Px, Py, Pz, Lx, Ly, Lz
+constexpr int kChunkTiles = 64; // record-reduction chunk, in 32-atom tiles
+constexpr int kIdxBits = 27;
+constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
+constexpr long long kSpinLimit = 20000000;  // ~2 s of 100 ns sleeps
+
+struct RepDev {
+  int64_t atom0;
+  int32_t n, npad;
+  int32_t cellbase, ncells;  // cell arrays: [cellbase, cellbase + ncells] (last entry is the sentinel)
+  int32_t nc[3];
+  int32_t tile0, ntiles;
+  int32_t chunk0, nchunks;
+  double L[3], cs[3];
+  float csf[3];
+  float pad0;
+  double dt, hdt, hs2, rl2;
+};
+
+struct FFDev {
+  int ns, lj, dsf, pad;
+  float lj_eps4[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float lj_eps24[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float lj_sig2[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float lj_rc2[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float lj_ushift[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float qqk[ACS_MAX_SPECIES * ACS_MAX_SPECIES];
+  float dsf_a, dsf_rc, dsf_rc2, dsf_c, dsf_erc_rc, dsf_fshift;
+  double self_e[ACS_MAX_SPECIES];   // k q^2 (erc/(2 rc) + a/sqrt(pi)) per species
+  double mass[ACS_MAX_SPECIES], inv_mass[ACS_MAX_SPECIES];
+};
+
+struct Eng {
+  int32_t R, maxnb;
+  int64_t S;  // slots
+  int32_t T, C, nchunks_total;
+  RepDev* rep;
+  int32_t* active;
+  int32_t* flag;
+  double *u, *v, *u0, *acc;
+  float4* img[2];
+  int32_t *cellid, *id, *sp;
+  int32_t *nbr, *nnb;
+  int32_t *tile_rep, *cell_rep;
+  int32_t *chunk_rep, *chunk_tile0, *chunk_ntiles;
+  double *xa, *tmp_xa, *tmp_v;
+  int32_t *tmp_cell, *tmp_id, *tmp_sp, *newcell, *perm;
+  int32_t *count, *start, *cursor;
+  double *partials, *chunk_part, *rec;
+  int32_t rec_cap;
+  acs_dev_status* status;
+  unsigned int* bar;  // [0] counter, [1] generation
+};
+
+__device__ __forceinline__ double py_mod(double x, double L) {
+  double r = fmod(x, L);
+  if (r != 0.0) {
+    if ((L < 0.0) != (r < 0.0)) r = add(r, L);
+  } else {
+    r = copysign(0.0, L);
+  }
+  return r;
+}
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+__device__ __forceinline__ float4 make_img(double ux, double uy, double uz, int sp) {
+  return make_float4((float)ux, (float)uy, (float)uz, __int_as_float(sp));
+}
+
+__device__ __forceinline__ void cell_coords(int local, const RepDev& R, int& c0, int& c1, int& c2) {
+  c2 = local % R.nc[2];
+  c1 = (local / R.nc[2]) % R.nc[1];
+  c0 = local / (R.nc[2] * R.nc[1]);
+}
+
+// ------------------------------------------------------------------------ bounded grid barrier --
+__device__ bool grid_sync(unsigned int* bar, acs_dev_status* st) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = bar + 1;
+    const unsigned int gen = *vgen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
+    ok = 1;
+    if (arrived == gridDim.x) {
+      bar[0] = 0u;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*vgen == gen) {
+        if (++it > kSpinLimit) {
+          atomicOr(&st->flags, ACS_FLAG_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// ------------------------------------------------------------------------------- pair kernel --
+// MODE 0: step (force, kick, record?, kick, drift, image, skin test); 1: last step of a block (force,
+// kick, record?, store acceleration); 2: force only (acceleration + records, no kicks).
+template <bool LJ, bool DSF, bool REC, int MODE>
+__global__ void __launch_bounds__(256) k_step(Eng E, FFDev ff, int src, int dst) {
+  __shared__ float4 shift_tab[8][27];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
+  const float4* __restrict__ imgs = E.img[src];
+  int cur_rep = -1;
+  for (int tile = blockIdx.x * wpb + wib; tile < E.T; tile += gridDim.x * wpb) {
+    const int r = E.tile_rep[tile];
+    if (!E.active[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (r != cur_rep) {
+      __syncwarp();
+      if (lane < 27) {
+        const int mx = lane % 3 - 1, my = (lane / 3) % 3 - 1, mz = lane / 9 - 1;
+        shift_tab[wib][lane] = make_float4(mx * R.csf[0], my * R.csf[1], mz * R.csf[2], 0.f);
+      }
+      __syncwarp();
+      cur_rep = r;
+    }
+    const int64_t i = (int64_t)tile * 32 + lane;
+    const bool valid = (i - R.atom0) < R.n;
+    double rv[kRecW] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (valid) {
+      const float4 pi = imgs[i];
+      const int si = __float_as_int(pi.w);
+      const int sio = si * ACS_MAX_SPECIES;
+      float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, eu = 0.f, ce = 0.f;
+      const int m = E.nnb[i];
+      const int32_t* __restrict__ lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
+#pragma unroll 2
+      for (int k = 0; k < m; ++k) {
+        const uint32_t e = (uint32_t)__ldg(lst + (int64_t)k * 32);
+        const float4 pj = __ldg(imgs + (e & kIdxMask));
+        const float4 sh = shift_tab[wib][e >> kIdxBits];
+        const float dx = (pj.x - pi.x) + sh.x;
+        const float dy = (pj.y - pi.y) + sh.y;
+        const float dz = (pj.z - pi.z) + sh.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const int p = sio + __float_as_int(pj.w);
+        float coef = 0.f;  // f_i += coef * d
+        if (LJ) {
+          if (r2 < ff.lj_rc2[p]) {
+            const float ir2 = 1.0f / r2;
+            const float sr2 = ff.lj_sig2[p] * ir2;
+            const float sr6 = sr2 * sr2 * sr2;
+            coef = -ff.lj_eps24[p] * ir2 * sr6 * (2.0f * sr6 - 1.0f);
+            if (REC) kahan_add(eu, ce, ff.lj_eps4[p] * (sr6 * sr6 - sr6) - ff.lj_ushift[p]);
+          }
+        }
+        if (DSF) {
+          if (r2 < ff.dsf_rc2) {
+            const float rr = sqrtf(r2);
+            const float ir = 1.0f / rr;
+            const float ar = ff.dsf_a * rr;
+            const float er = erfcf(ar);
+            const float qq = ff.qqk[p];
+            coef -= qq * ((er * ir * ir + ff.dsf_c * __expf(-ar * ar) * ir) - ff.dsf_fshift) * ir;
+            if (REC) kahan_add(eu, ce, qq * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
+          }
+        }
+        kahan_add(fx, cx, coef * dx);
+        kahan_add(fy, cy, coef * dy);
+        kahan_add(fz, cz, coef * dz);
+      }
+      const double im = ff.inv_mass[si];
+      const double ax = ((double)fx - (double)cx) * im;
+      const double ay = ((double)fy - (double)cy) * im;
+      const double az = ((double)fz - (double)cz) * im;
+      if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
+      double vx = E.v[3 * i], vy = E.v[3 * i + 1], vz = E.v[3 * i + 2];
+      if (MODE != 2) {
+        vx += R.hdt * ax;
+        vy += R.hdt * ay;
+        vz += R.hdt * az;
+      }
+      if (REC) {
+        const double ms = ff.mass[si];
+        rv[0] = 0.5 * ms * (vx * vx + vy * vy + vz * vz);
+        rv[1] = 0.5 * ((double)eu - (double)ce) - (DSF ? ff.self_e[si] : 0.0);
+        const double px = ms * vx, py = ms * vy, pz = ms * vz;
+        rv[2] = px;
+        rv[3] = py;
+        rv[4] = pz;
+        int c0, c1, c2;
+        cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
+        const double x = py_mod(c0 * R.cs[0] + E.u[3 * i], R.L[0]);
+        const double y = py_mod(c1 * R.cs[1] + E.u[3 * i + 1], R.L[1]);
+        const double z = py_mod(c2 * R.cs[2] + E.u[3 * i + 2], R.L[2]);
+        rv[5] = y * pz - z * py;
+        rv[6] = z * px - x * pz;
+        rv[7] = x * py - y * px;
+      }
+      if (MODE == 0) {
+        vx += R.hdt * ax;
+        vy += R.hdt * ay;
+        vz += R.hdt * az;
+        const double ux = E.u[3 * i] + R.dt * vx, uy = E.u[3 * i + 1] + R.dt * vy, uz = E.u[3 * i + 2] + R.dt * vz;
+        E.u[3 * i] = ux;
+        E.u[3 * i + 1] = uy;
+        E.u[3 * i + 2] = uz;
+        E.img[dst][i] = make_img(ux, uy, uz, si);
+        const double ddx = ux - E.u0[3 * i], ddy = uy - E.u0[3 * i + 1], ddz = uz - E.u0[3 * i + 2];
+        if (!(ddx * ddx + ddy * ddy + ddz * ddz < R.hs2)) E.flag[r] = 1;
+      } else {
+        E.acc[3 * i] = ax;
+        E.acc[3 * i + 1] = ay;
+        E.acc[3 * i + 2] = az;
+      }
+      if (MODE != 2) {
+        E.v[3 * i] = vx;
+        E.v[3 * i + 1] = vy;
+        E.v[3 * i + 2] = vz;
+      }
+    }
+    if (REC) {
+#pragma unroll
+      for (int w = 0; w < kRecW; ++w) {
+        double x = rv[w];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) E.partials[(int64_t)tile * kRecW + w] = x;
+      }
+    }
+  }
+}
+
+// Prologue of a block: first half-kick and drift from the stored accelerations, image, skin test.
+__global__ void k_prologue(Eng E, int dst) {
+  if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E.S; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[i >> 5];
+    if (!E.active[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (i - R.atom0 >= R.n) continue;
+    double vx = E.v[3 * i] + R.hdt * E.acc[3 * i];
+    double vy = E.v[3 * i + 1] + R.hdt * E.acc[3 * i + 1];
+    double vz = E.v[3 * i + 2] + R.hdt * E.acc[3 * i + 2];
+    const double ux = E.u[3 * i] + R.dt * vx, uy = E.u[3 * i + 1] + R.dt * vy, uz = E.u[3 * i + 2] + R.dt * vz;
+    E.v[3 * i] = vx;
+    E.v[3 * i + 1] = vy;
+    E.v[3 * i + 2] = vz;
+    E.u[3 * i] = ux;
+    E.u[3 * i + 1] = uy;
+    E.u[3 * i + 2] = uz;
+    E.img[dst][i] = make_img(ux, uy, uz, E.sp[i]);
+    const double ddx = ux - E.u0[3 * i], ddy = uy - E.u0[3 * i + 1], ddz = uz - E.u0[3 * i + 2];
+    if (!(ddx * ddx + ddy * ddy + ddz * ddz < R.hs2)) E.flag[r] = 1;
+  }
+}
+
+__device__ __forceinline__ void stencil(int c, int nc, int& lo, int& hi) {
+  if (nc >= 3) {
+    lo = -1;
+    hi = 1;
+  } else {
+    lo = 0;
+    hi = 0;
+  }
+}
+
+__device__ __forceinline__ int wrapc(int c, int nc) { return c < 0 ? c + nc : (c >= nc ? c - nc : c); }
+
+__device__ int block_scan_excl(int v, int* total) {
+  __shared__ int ws[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const int ex = x - v + (wid ? ws[wid - 1] : 0);
+  *total = ws[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return ex;
+}
+
+// Rebuild of flagged replicas and per-replica record reduction. Cooperative launch (all blocks resident);
+// every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging.
+__global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
+  __shared__ unsigned char fl[kMaxRep];
+  __shared__ int any_s;
+  if (threadIdx.x == 0) any_s = 0;
+  __syncthreads();
+  int local_any = 0;
+  for (int r = threadIdx.x; r < E.R; r += blockDim.x) {
+    const unsigned char f = (E.active[r] && (force_all || E.flag[r])) ? 1 : 0;
+    fl[r] = f;
+    local_any |= f;
+  }
+  if (local_any) atomicOr(&any_s, 1);
+  __syncthreads();
+  const bool any = any_s != 0;
+  const bool err0 = (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) != 0;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+
+  if (rec && !err0) {
+    // Q1: chunk partials (fixed chunking => deterministic)
+    for (int c = blockIdx.x; c < E.nchunks_total; c += gridDim.x) {
+      if (!E.active[E.chunk_rep[c]]) continue;
+      if (threadIdx.x < kRecW) {
+        double s = 0.0;
+        const int t0 = E.chunk_tile0[c], nt = E.chunk_ntiles[c];
+        for (int t = 0; t < nt; ++t) s += E.partials[(int64_t)(t0 + t) * kRecW + threadIdx.x];
+        E.chunk_part[(int64_t)c * kRecW + threadIdx.x] = s;
+      }
+    }
+    if (!grid_sync(E.bar, E.status)) return;
+    // Q2: per-replica sum of its chunks in order
+    for (int r = blockIdx.x; r < E.R; r += gridDim.x) {
+      if (!E.active[r] || threadIdx.x >= kRecW) continue;
+      const RepDev& R = E.rep[r];
+      double s = 0.0;
+      for (int c = 0; c < R.nchunks; ++c) s += E.chunk_part[(int64_t)(R.chunk0 + c) * kRecW + threadIdx.x];
+      if (rec_idx < E.rec_cap) E.rec[((int64_t)rec_idx * E.R + r) * kRecW + threadIdx.x] = s;
+    }
+  }
+  if (!any || err0) return;
+  if (!grid_sync(E.bar, E.status)) return;  // every block has read the flags before they are cleared
+
+  // P0: clear counters of flagged replicas' cells
+  for (int64_t c = gtid; c < E.C; c += gstride) {
+    if (fl[E.cell_rep[c]]) {
+      E.count[c] = 0;
+      E.cursor[c] = 0;
+    }
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P1: absolute wrapped positions and new cells
+  for (int64_t s = gtid; s < E.S; s += gstride) {
+    const int r = E.tile_rep[s >> 5];
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (s - R.atom0 >= R.n) continue;
+    int c0, c1, c2;
+    cell_coords(E.cellid[s] - R.cellbase, R, c0, c1, c2);
+    const double o[3] = {c0 * R.cs[0], c1 * R.cs[1], c2 * R.cs[2]};
+    int nc3[3];
+    double x[3];
+    bool fin = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      x[d] = py_mod(o[d] + E.u[3 * s + d], R.L[d]);
+      fin &= isfinite(x[d]);
+      // cell = clip(int(x / L * nc), 0, nc - 1)  (accusim/forces.py:290-291)
+      const double t = mul(div(x[d], R.L[d]), (double)R.nc[d]);
+      nc3[d] = !(t >= 1.0) ? 0 : (t >= (double)(R.nc[d] - 1) ? R.nc[d] - 1 : (int)t);
+      E.xa[3 * s + d] = x[d];
+    }
+    if (!fin) {
+      atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
+      nc3[0] = nc3[1] = nc3[2] = 0;
+    }
+    const int c = R.cellbase + (nc3[0] * R.nc[1] + nc3[1]) * R.nc[2] + nc3[2];
+    E.newcell[s] = c;
+    atomicAdd(&E.count[c], 1);
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P2: per-replica exclusive scan of cell counts -> slot starts; clear flags; count rebuilds
+  for (int r = blockIdx.x; r < E.R; r += gridDim.x) {
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    int carry = 0;
+    for (int b = 0; b < R.ncells; b += blockDim.x) {
+      const int c = b + threadIdx.x;
+      const int v = c < R.ncells ? E.count[R.cellbase + c] : 0;
+      int total;
+      const int ex = block_scan_excl(v, &total);
+      if (c < R.ncells) E.start[R.cellbase + c] = (int32_t)(R.atom0 + carry + ex);
+      carry += total;
+    }
+    if (threadIdx.x == 0) {
+      E.start[R.cellbase + R.ncells] = (int32_t)(R.atom0 + R.n);
+      E.flag[r] = 0;
+      atomicAdd(&E.status->rebuilds, 1);
+    }
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P3: scatter old slots to new slots
+  for (int64_t s = gtid; s < E.S; s += gstride) {
+    const int r = E.tile_rep[s >> 5];
+    if (!fl[r] || s - E.rep[r].atom0 >= E.rep[r].n) continue;
+    const int c = E.newcell[s];
+    E.perm[E.start[c] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P3b: deterministic order inside each cell (ascending old slot)
+  for (int64_t c = gtid; c < E.C; c += gstride) {
+    const int r = E.cell_rep[c];
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (c == R.cellbase + R.ncells) continue;  // sentinel
+    const int a0 = E.start[c], a1 = E.start[c + 1];
+    for (int a = a0 + 1; a < a1; ++a) {
+      const int v = E.perm[a];
+      int b = a - 1;
+      while (b >= a0 && E.perm[b] > v) {
+        E.perm[b + 1] = E.perm[b];
+        --b;
+      }
+      E.perm[b + 1] = v;
+    }
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P4: gather into new order
+  for (int64_t k = gtid; k < E.S; k += gstride) {
+    const int r = E.tile_rep[k >> 5];
+    if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
+    const int o = E.perm[k];
+    E.tmp_cell[k] = E.newcell[o];
+    E.tmp_id[k] = E.id[o];
+    E.tmp_sp[k] = E.sp[o];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      E.tmp_xa[3 * k + d] = E.xa[3 * o + d];
+      E.tmp_v[3 * k + d] = E.v[3 * o + d];
+    }
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P5: commit; offsets from the new cell origins; images
+  for (int64_t k = gtid; k < E.S; k += gstride) {
+    const int r = E.tile_rep[k >> 5];
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (k - R.atom0 >= R.n) continue;
+    const int c = E.tmp_cell[k];
+    int c0, c1, c2;
+    cell_coords(c - R.cellbase, R, c0, c1, c2);
+    const double ux = E.tmp_xa[3 * k] - c0 * R.cs[0];
+    const double uy = E.tmp_xa[3 * k + 1] - c1 * R.cs[1];
+    const double uz = E.tmp_xa[3 * k + 2] - c2 * R.cs[2];
+    E.cellid[k] = c;
+    E.id[k] = E.tmp_id[k];
+    E.sp[k] = E.tmp_sp[k];
+    E.u[3 * k] = ux;
+    E.u[3 * k + 1] = uy;
+    E.u[3 * k + 2] = uz;
+    E.u0[3 * k] = ux;
+    E.u0[3 * k + 1] = uy;
+    E.u0[3 * k + 2] = uz;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) E.v[3 * k + d] = E.tmp_v[3 * k + d];
+    E.img[dst][k] = make_img(ux, uy, uz, E.tmp_sp[k]);
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  // P6: neighbour lists with the reference's FP64 filter; image shift codes
+  for (int64_t i = gtid; i < E.S; i += gstride) {
+    const int r = E.tile_rep[i >> 5];
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (i - R.atom0 >= R.n) continue;
+    int c0, c1, c2;
+    cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
+    const double xi = E.tmp_xa[3 * i], yi = E.tmp_xa[3 * i + 1], zi = E.tmp_xa[3 * i + 2];
+    const double uxi = E.u[3 * i], uyi = E.u[3 * i + 1], uzi = E.u[3 * i + 2];
+    int lo0, hi0, lo1, hi1, lo2, hi2;
+    stencil(c0, R.nc[0], lo0, hi0);
+    stencil(c1, R.nc[1], lo1, hi1);
+    stencil(c2, R.nc[2], lo2, hi2);
+    int cnt = 0;
+    bool bad = false;
+    int32_t* lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
+    for (int a = lo0; a <= hi0; ++a) {
+      const int n0 = wrapc(c0 + a, R.nc[0]);
+      for (int b = lo1; b <= hi1; ++b) {
+        const int n1 = wrapc(c1 + b, R.nc[1]);
+        for (int d = lo2; d <= hi2; ++d) {
+          const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + wrapc(c2 + d, R.nc[2]);
+          for (int k = E.start[cc], ke = E.start[cc + 1]; k < ke; ++k) {
+            if (k == i) continue;
+            double dx = sub(E.tmp_xa[3 * k], xi), dy = sub(E.tmp_xa[3 * k + 1], yi), dz = sub(E.tmp_xa[3 * k + 2], zi);
+            dx = min_image(dx, R.L[0]);
+            dy = min_image(dy, R.L[1]);
+            dz = min_image(dz, R.L[2]);
+            if (norm2(dx, dy, dz) < R.rl2) {
+              const int mx = (int)rint((dx - (E.u[3 * k] - uxi)) / R.cs[0]);
+              const int my = (int)rint((dy - (E.u[3 * k + 1] - uyi)) / R.cs[1]);
+              const int mz = (int)rint((dz - (E.u[3 * k + 2] - uzi)) / R.cs[2]);
+              const bool out = (mx < -1 || mx > 1 || my < -1 || my > 1 || mz < -1 || mz > 1);
+              bad |= out;  // reported as an error; the stored code stays inside the 27-entry shift table
+              const uint32_t code = out ? 13u : (uint32_t)((mx + 1) + 3 * (my + 1) + 9 * (mz + 1));
+              if (cnt < E.maxnb) lst[(int64_t)cnt * 32] = (int32_t)((uint32_t)k | (code << kIdxBits));
+              ++cnt;
+            }
+          }
+        }
+      }
+    }
+    E.nnb[i] = min(cnt, E.maxnb);
+    if (cnt > E.maxnb) {
+      atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
+      atomicMax(&E.status->need_nbr, cnt);
+    }
+    if (bad) atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
+  }
+}
+
+// Scatter caller arrays (replica-concatenated, engine units) into slots; cell 0 origin so u = x.
+__global__ void k_load(Eng E, const double* __restrict__ pos, const double* __restrict__ vel,
+                       const int32_t* __restrict__ sp, const int64_t* __restrict__ src0) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < E.S; s += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[s >> 5];
+    const RepDev& R = E.rep[r];
+    const int64_t loc = s - R.atom0;
+    if (loc >= R.n) {
+      for (int d = 0; d < 3; ++d) E.u[3 * s + d] = E.v[3 * s + d] = E.u0[3 * s + d] = E.acc[3 * s + d] = 0.0;
+      E.id[s] = -1;
+      E.sp[s] = 0;
+      E.cellid[s] = R.cellbase;
+      E.nnb[s] = 0;
+      E.img[0][s] = E.img[1][s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
+    }
+    const int64_t g = src0[r] + loc;
+    for (int d = 0; d < 3; ++d) {
+      E.u[3 * s + d] = pos[3 * g + d];
+      E.v[3 * s + d] = vel[3 * g + d];
+      E.acc[3 * s + d] = 0.0;
+    }
+    E.id[s] = (int32_t)loc;
+    E.sp[s] = sp[g];
+    E.cellid[s] = R.cellbase;
+  }
+}
+
+// Gather slots back to caller order: absolute wrapped positions, velocities, accelerations.
+__global__ void k_store(Eng E, double* __restrict__ pos, double* __restrict__ vel, double* __restrict__ acc,
+                        const int64_t* __restrict__ src0) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < E.S; s += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[s >> 5];
+    const RepDev& R = E.rep[r];
+    if (s - R.atom0 >= R.n) continue;
+    const int64_t g = src0[r] + E.id[s];
+    int c0, c1, c2;
+    cell_coords(E.cellid[s] - R.cellbase, R, c0, c1, c2);
+    const double o[3] = {c0 * R.cs[0], c1 * R.cs[1], c2 * R.cs[2]};
+    for (int d = 0; d < 3; ++d) {
+      if (pos) pos[3 * g + d] = py_mod(o[d] + E.u[3 * s + d], R.L[d]);
+      if (vel) vel[3 * g + d] = E.v[3 * s + d];
+      if (acc) acc[3 * g + d] = E.acc[3 * s + d];
+    }
+  }
+}
+
+// Load caller-order state into the current slots without re-binning: offsets stay continuous (minimum
+// image against the current offset), so the next block's skin test decides whether the list survives.
+__global__ void k_load_keep(Eng E, const double* __restrict__ pos, const double* __restrict__ vel,
+                            const int64_t* __restrict__ src0) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < E.S; s += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[s >> 5];
+    const RepDev& R = E.rep[r];
+    if (s - R.atom0 >= R.n) continue;
+    const int64_t g = src0[r] + E.id[s];
+    int c0, c1, c2;
+    cell_coords(E.cellid[s] - R.cellbase, R, c0, c1, c2);
+    const double o[3] = {c0 * R.cs[0], c1 * R.cs[1], c2 * R.cs[2]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double uo = E.u[3 * s + d];
+      double du = (pos[3 * g + d] - o[d]) - uo;
+      du -= R.L[d] * rint(du / R.L[d]);
+      E.u[3 * s + d] = uo + du;
+      E.v[3 * s + d] = vel[3 * g + d];
+    }
+  }
+}
+
+// Unique pairs inside the physical cutoffs (LJ r < cutoff sigma_ij, DSF r < rc), by the step kernel's
+// FP32 test on the current images: the unit of work for the roofline.
+__global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out) {
+  unsigned long long nl = 0, nd = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E.S; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[i >> 5];
+    const RepDev& R = E.rep[r];
+    if (i - R.atom0 >= R.n) continue;
+    const float4 pi = E.img[src][i];
+    const int sio = __float_as_int(pi.w) * ACS_MAX_SPECIES;
+    const int32_t* lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
+    for (int k = 0; k < E.nnb[i]; ++k) {
+      const uint32_t e = (uint32_t)lst[(int64_t)k * 32];
+      const float4 pj = E.img[src][e & kIdxMask];
+      const uint32_t code = e >> kIdxBits;
+      const int mx = (int)(code % 3) - 1, my = (int)((code / 3) % 3) - 1, mz = (int)(code / 9) - 1;
+      const float dx = (pj.x - pi.x) + mx * R.csf[0];
+      const float dy = (pj.y - pi.y) + my * R.csf[1];
+      const float dz = (pj.z - pi.z) + mz * R.csf[2];
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      const int p = sio + __float_as_int(pj.w);
+      if (ff.lj && r2 < ff.lj_rc2[p]) ++nl;
+      if (ff.dsf && r2 < ff.dsf_rc2) ++nd;
+    }
+  }
+  atomicAdd(out, nl);
+  atomicAdd(out + 1, nd);
+}
+
+inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// ====================================================================================== host side ==
+struct acs_engine {
+  Eng E;
+  FFDev ff;
+  std::vector<RepDev> reps;
+  std::vector<int64_t> src0;
+  int64_t* src0_dev = nullptr;
+  int coop_blocks = 0;
+  int step_blocks = 0;
+  int step_threads = 256;
+  int n_lj = 0, n_dsf = 0;
+  std::map<long long, cudaGraphExec_t> graphs;
+  int dev = 0;
+};
+
+namespace {
+
+struct Layout {
+  size_t off[64];
+  int k = 0;
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    off[k] = total;
+    total += a256(bytes);
+    return k++;
+  }
+};
+
+void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<int64_t>& src0, int64_t& S, int32_t& T,
+          int32_t& C, int32_t& NCH, int& err) {
+  err = ACS_OK;
+  reps.clear();
+  src0.clear();
+  S = 0;
+  T = 0;
+  C = 0;
+  NCH = 0;
+  int64_t g = 0;
+  for (int r = 0; r < cfg->n_replicas; ++r) {
+    const acs_replica& q = cfg->replicas[r];
+    RepDev R{};
+    if (q.n < 1 || !(q.rlist > 0.0) || !(q.half_skin >= 0.0) || !(q.dt > 0.0)) {
+      err = ACS_ERR_ARG;
+      return;
+    }
+    R.atom0 = S;
+    R.n = q.n;
+    R.npad = (q.n + 31) / 32 * 32;
+    int64_t ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+      if (!(q.box[d] > 0.0)) {
+        err = ACS_ERR_ARG;
+        return;
+      }
+      // cells no narrower than the list radius (so the 27-cell stencil is complete), at most 1024 per edge
+      double f = floor(q.box[d] / q.rlist);
+      int nc = f < 1.0 ? 1 : (int)std::min(f, 1024.0);
+      while (nc > 1 && q.box[d] / nc < q.rlist) --nc;
+      if (nc < 3) nc = 1;
+      R.nc[d] = nc;
+      R.L[d] = q.box[d];
+      R.cs[d] = q.box[d] / nc;
+      R.csf[d] = (float)R.cs[d];
+      ncell *= nc;
+      if (q.rlist * 2.0 >= q.box[d]) err = ACS_ERR_UNSUPPORTED;  // minimum image needs rlist < box/2
+    }
+    if (err) return;
+    R.cellbase = C;
+    R.ncells = (int32_t)ncell;
+    R.tile0 = (int32_t)(S / 32);
+    R.ntiles = R.npad / 32;
+    R.chunk0 = NCH;
+    R.nchunks = (R.ntiles + kChunkTiles - 1) / kChunkTiles;
+    R.dt = q.dt;
+    R.hdt = 0.5 * q.dt;
+    R.hs2 = q.half_skin * q.half_skin;
+    R.rl2 = q.rlist * q.rlist;
+    reps.push_back(R);
+    src0.push_back(g);
+    g += q.n;
+    S += R.npad;
+    C += (int32_t)ncell + 1;
+    NCH += R.nchunks;
+    T = (int32_t)(S / 32);
+    if (S >= (int64_t)kIdxMask || C > INT32_MAX / 2) {
+      err = ACS_ERR_UNSUPPORTED;
+      return;
+    }
+  }
+}
+
+Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int32_t maxnb, int32_t rec_cap) {
+  Layout L;
+  L.add(sizeof(RepDev) * R);                 // 0 rep
+  L.add(4 * (size_t)R);                      // 1 active
+  L.add(4 * (size_t)R);                      // 2 flag
+  L.add(24 * (size_t)S);                     // 3 u
+  L.add(24 * (size_t)S);                     // 4 v
+  L.add(24 * (size_t)S);                     // 5 u0
+  L.add(24 * (size_t)S);                     // 6 acc
+  L.add(16 * (size_t)S);                     // 7 img0
+  L.add(16 * (size_t)S);                     // 8 img1
+  L.add(4 * (size_t)S);                      // 9 cellid
+  L.add(4 * (size_t)S);                      // 10 id
+  L.add(4 * (size_t)S);                      // 11 sp
+  L.add(4 * (size_t)S * maxnb);              // 12 nbr
+  L.add(4 * (size_t)S);                      // 13 nnb
+  L.add(4 * (size_t)T);                      // 14 tile_rep
+  L.add(4 * (size_t)C);                      // 15 cell_rep
+  L.add(4 * (size_t)NCH);                    // 16 chunk_rep
+  L.add(4 * (size_t)NCH);                    // 17 chunk_tile0
+  L.add(4 * (size_t)NCH);                    // 18 chunk_ntiles
+  L.add(24 * (size_t)S);                     // 19 xa
+  L.add(24 * (size_t)S);                     // 20 tmp_xa
+  L.add(24 * (size_t)S);                     // 21 tmp_v
+  L.add(4 * (size_t)S);                      // 22 tmp_cell
+  L.add(4 * (size_t)S);                      // 23 tmp_id
+  L.add(4 * (size_t)S);                      // 24 tmp_sp
+  L.add(4 * (size_t)S);                      // 25 newcell
+  L.add(4 * (size_t)S);                      // 26 perm
+  L.add(4 * (size_t)C);                      // 27 count
+  L.add(4 * (size_t)C);                      // 28 start
+  L.add(4 * (size_t)C);                      // 29 cursor
+  L.add(8 * (size_t)T * kRecW);              // 30 partials
+  L.add(8 * (size_t)NCH * kRecW);            // 31 chunk partials
+  L.add(8 * (size_t)rec_cap * R * kRecW);    // 32 records
+  L.add(sizeof(acs_dev_status));             // 33 status
+  L.add(16);                                 // 34 barrier
+  L.add(8 * (size_t)R);                      // 35 src0
+  return L;
+}
+
+FFDev make_ff(const acs_forcefield& f, int& err) {
+  FFDev ff{};
+  err = ACS_OK;
+  if (f.n_species < 1 || f.n_species > ACS_MAX_SPECIES || (!f.lj && !f.dsf)) {
+    err = ACS_ERR_ARG;
+    return ff;
+  }
+  const int S = ACS_MAX_SPECIES;
+  ff.ns = f.n_species;
+  ff.lj = f.lj;
+  ff.dsf = f.dsf;
+  for (int a = 0; a < f.n_species; ++a) {
+    if (!(f.mass[a] > 0.0)) err = ACS_ERR_ARG;
+    ff.mass[a] = f.mass[a];
+    ff.inv_mass[a] = 1.0 / f.mass[a];
+  }
+  const double c6 = 1.0 / (f.lj_cutoff * f.lj_cutoff);
+  const double src6 = c6 * c6 * c6;
+  for (int a = 0; a < f.n_species; ++a)
+    for (int b = 0; b < f.n_species; ++b) {
+      const int p = a * S + b, q = a * f.n_species + b;
+      const double e = f.lj ? f.lj_eps[q] : 0.0, s = f.lj ? f.lj_sig[q] : 1.0;
+      ff.lj_eps4[p] = (float)(4.0 * e);
+      ff.lj_eps24[p] = (float)(24.0 * e);
+      ff.lj_sig2[p] = (float)(s * s);
+      ff.lj_rc2[p] = e > 0.0 ? (float)((f.lj_cutoff * s) * (f.lj_cutoff * s)) : 0.f;
+      ff.lj_ushift[p] = (float)(4.0 * e * (src6 * src6 - src6));
+      ff.qqk[p] = f.dsf ? (float)(f.dsf_k * f.q[a] * f.q[b]) : 0.f;
+    }
+  if (f.dsf) {
+    const double a = f.dsf_alpha, rc = f.dsf_rcut;
+    const double c = 2.0 * a / sqrt(M_PI);
+    const double erc = erfc(a * rc);
+    const double fshift = erc / (rc * rc) + c * exp(-(a * rc) * (a * rc)) / rc;
+    ff.dsf_a = (float)a;
+    ff.dsf_rc = (float)rc;
+    ff.dsf_rc2 = (float)(rc * rc);
+    ff.dsf_c = (float)c;
+    ff.dsf_erc_rc = (float)(erc / rc);
+    ff.dsf_fshift = (float)fshift;
+    for (int s = 0; s < f.n_species; ++s) ff.self_e[s] = f.dsf_k * f.q[s] * f.q[s] * (erc / (2.0 * rc) + a / sqrt(M_PI));
+  }
+  return ff;
+}
+
+template <bool LJ, bool DSF>
+int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
+  dim3 g(e->step_blocks), b(e->step_threads);
+  if (mode == 0) {
+    if (rec) k_step<LJ, DSF, true, 0><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    else k_step<LJ, DSF, false, 0><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+  } else if (mode == 1) {
+    if (rec) k_step<LJ, DSF, true, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    else k_step<LJ, DSF, false, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+  } else {
+    k_step<LJ, DSF, true, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+  }
+  return launch_status();
+}
+
+int launch_step(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
+  if (e->ff.lj && e->ff.dsf) return launch_step_t<true, true>(e, rec, mode, src, dst, s);
+  if (e->ff.lj) return launch_step_t<true, false>(e, rec, mode, src, dst, s);
+  return launch_step_t<false, true>(e, rec, mode, src, dst, s);
+}
+
+int launch_rebuild(acs_engine* e, int dst, int rec, int rec_idx, int force_all, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(e->coop_blocks);
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t err = cudaLaunchKernelEx(&cfg, k_rebuild, e->E, dst, rec, rec_idx, force_all);
+  return err == cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
+}
+
+// A block of `steps` steps: prologue, rebuild check, then (step, rebuild check) x steps; records at the
+// steps whose bit is set in rec_mask (bit k = step k of the block, 0-based); the last step stores the
+// accelerations. Image buffers alternate 0,1.
+int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cudaStream_t s) {
+  int st = ACS_OK;
+  k_prologue<<<e->step_blocks, 256, 0, s>>>(e->E, 0);
+  if ((st = launch_status())) return st;
+  if ((st = launch_rebuild(e, 0, 0, 0, 0, s))) return st;
+  int rec_idx = 0;
+  for (int k = 0; k < steps; ++k) {
+    const int src = k & 1, dst = (k + 1) & 1;
+    const bool last = (k == steps - 1);
+    const int rec = rec_at[k] ? 1 : 0;
+    if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, s))) return st;
+    if (!last || rec) {
+      if ((st = launch_rebuild(e, dst, rec, rec_idx, 0, s))) return st;
+    }
+    rec_idx += rec;
+  }
+  return ACS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t acs_engine_bytes(const acs_engine_config* cfg) {
+  if (!cfg || cfg->n_replicas < 1 || cfg->n_replicas > kMaxRep || !cfg->replicas || cfg->maxnb < 1) return 0;
+  std::vector<RepDev> reps;
+  std::vector<int64_t> src0;
+  int64_t S;
+  int32_t T, C, NCH;
+  int err;
+  plan(cfg, reps, src0, S, T, C, NCH, err);
+  if (err) return 0;
+  return make_layout(cfg->n_replicas, S, T, C, NCH, cfg->maxnb, std::max(cfg->rec_cap, 1)).total;
+}
+
+int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs_engine** out) {
+  if (!cfg || !out || !mem || cfg->n_replicas < 1 || cfg->n_replicas > kMaxRep || !cfg->replicas || cfg->maxnb < 1 ||
+      cfg->maxnb > 4096)
+    return ACS_ERR_ARG;
+  if ((uintptr_t)mem & 255) return ACS_ERR_ARG;
+  acs_engine* e = new acs_engine();
+  int64_t S;
+  int32_t T, C, NCH;
+  int err;
+  plan(cfg, e->reps, e->src0, S, T, C, NCH, err);
+  if (err) {
+    delete e;
+    return err;
+  }
+  e->ff = make_ff(cfg->ff, err);
+  if (err) {
+    delete e;
+    return err;
+  }
+  const int rec_cap = std::max(cfg->rec_cap, 1);
+  Layout L = make_layout(cfg->n_replicas, S, T, C, NCH, cfg->maxnb, rec_cap);
+  if (bytes < L.total) {
+    delete e;
+    return ACS_ERR_WORKSPACE;
+  }
+  char* b = (char*)mem;
+  Eng& E = e->E;
+  E.R = cfg->n_replicas;
+  E.maxnb = cfg->maxnb;
+  E.S = S;
+  E.T = T;
+  E.C = C;
+  E.nchunks_total = NCH;
+  E.rec_cap = rec_cap;
+  E.rep = (RepDev*)(b + L.off[0]);
+  E.active = (int32_t*)(b + L.off[1]);
+  E.flag = (int32_t*)(b + L.off[2]);
+  E.u = (double*)(b + L.off[3]);
+  E.v = (double*)(b + L.off[4]);
+  E.u0 = (double*)(b + L.off[5]);
+  E.acc = (double*)(b + L.off[6]);
+  E.img[0] = (float4*)(b + L.off[7]);
+  E.img[1] = (float4*)(b + L.off[8]);
+  E.cellid = (int32_t*)(b + L.off[9]);
+  E.id = (int32_t*)(b + L.off[10]);
+  E.sp = (int32_t*)(b + L.off[11]);
+  E.nbr = (int32_t*)(b + L.off[12]);
+  E.nnb = (int32_t*)(b + L.off[13]);
+  E.tile_rep = (int32_t*)(b + L.off[14]);
+  E.cell_rep = (int32_t*)(b + L.off[15]);
+  E.chunk_rep = (int32_t*)(b + L.off[16]);
+  E.chunk_tile0 = (int32_t*)(b + L.off[17]);
+  E.chunk_ntiles = (int32_t*)(b + L.off[18]);
+  E.xa = (double*)(b + L.off[19]);
+  E.tmp_xa = (double*)(b + L.off[20]);
+  E.tmp_v = (double*)(b + L.off[21]);
+  E.tmp_cell = (int32_t*)(b + L.off[22]);
+  E.tmp_id = (int32_t*)(b + L.off[23]);
+  E.tmp_sp = (int32_t*)(b + L.off[24]);
+  E.newcell = (int32_t*)(b + L.off[25]);
+  E.perm = (int32_t*)(b + L.off[26]);
+  E.count = (int32_t*)(b + L.off[27]);
+  E.start = (int32_t*)(b + L.off[28]);
+  E.cursor = (int32_t*)(b + L.off[29]);
+  E.partials = (double*)(b + L.off[30]);
+  E.chunk_part = (double*)(b + L.off[31]);
+  E.rec = (double*)(b + L.off[32]);
+  E.status = (acs_dev_status*)(b + L.off[33]);
+  E.bar = (unsigned int*)(b + L.off[34]);
+  e->src0_dev = (int64_t*)(b + L.off[35]);
+
+  // host-built index tables
+  std::vector<int32_t> tile_rep(T), cell_rep(C), chunk_rep(NCH), chunk_t0(NCH), chunk_nt(NCH);
+  for (int r = 0; r < E.R; ++r) {
+    const RepDev& R = e->reps[r];
+    for (int t = 0; t < R.ntiles; ++t) tile_rep[R.tile0 + t] = r;
+    for (int c = 0; c <= R.ncells; ++c) cell_rep[R.cellbase + c] = r;
+    for (int c = 0; c < R.nchunks; ++c) {
+      chunk_rep[R.chunk0 + c] = r;
+      chunk_t0[R.chunk0 + c] = R.tile0 + c * kChunkTiles;
+      chunk_nt[R.chunk0 + c] = std::min(kChunkTiles, R.ntiles - c * kChunkTiles);
+    }
+  }
+  std::vector<int32_t> ones(E.R, 1), zeros(E.R, 0);
+  acs_dev_status st0{};
+  st0.fail_step = -1;
+  unsigned int bar0[4] = {0, 0, 0, 0};
+  bool ok = cudaGetDevice(&e->dev) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.rep, e->reps.data(), sizeof(RepDev) * E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.active, ones.data(), 4 * E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.flag, zeros.data(), 4 * E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.tile_rep, tile_rep.data(), 4 * (size_t)T, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.cell_rep, cell_rep.data(), 4 * (size_t)C, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.chunk_rep, chunk_rep.data(), 4 * (size_t)NCH, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.chunk_tile0, chunk_t0.data(), 4 * (size_t)NCH, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.chunk_ntiles, chunk_nt.data(), 4 * (size_t)NCH, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.status, &st0, sizeof(st0), cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.bar, bar0, 16, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(e->src0_dev, e->src0.data(), 8 * (size_t)E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemset(E.nnb, 0, 4 * (size_t)S) == cudaSuccess;
+  int sms = 0, per_sm = 0;
+  ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev) == cudaSuccess;
+  ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, 256, 0) == cudaSuccess;
+  if (!ok || per_sm < 1) {
+    delete e;
+    return ACS_ERR_CUDA;
+  }
+  e->coop_blocks = sms * std::min(per_sm, 2);
+  const int grid_mult = cfg->grid_mult > 0 ? cfg->grid_mult : 0;
+  const int64_t need = (S + 255) / 256;
+  e->step_blocks = (int)(grid_mult ? std::min<int64_t>(need, (int64_t)sms * grid_mult) : need);
+  if (e->step_blocks < 1) e->step_blocks = 1;
+  *out = e;
+  return ACS_OK;
+}
+
+int acs_engine_set_state(acs_engine* e, const double* pos, const double* vel, const int32_t* species, void* stream) {
+  if (!e || !pos || !vel || !species) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_load<<<e->step_blocks, 256, 0, s>>>(e->E, pos, vel, species, e->src0_dev);
+  int st = launch_status();
+  if (st) return st;
+  // build lists for every replica, then one force evaluation (accelerations + initial records)
+  if ((st = launch_rebuild(e, 0, 0, 0, 1, s))) return st;
+  if ((st = launch_step(e, 1, 2, 0, 0, s))) return st;
+  return launch_rebuild(e, 0, 1, 0, 0, s);
+}
+
+int acs_engine_get_state(acs_engine* e, double* pos, double* vel, double* acc, void* stream) {
+  if (!e) return ACS_ERR_ARG;
+  k_store<<<e->step_blocks, 256, 0, (cudaStream_t)stream>>>(e->E, pos, vel, acc, e->src0_dev);
+  return launch_status();
+}
+
+int acs_engine_set_active(acs_engine* e, const int32_t* active_host, void* stream) {
+  if (!e || !active_host) return ACS_ERR_ARG;
+  return cudaMemcpyAsync(e->E.active, active_host, 4 * (size_t)e->E.R, cudaMemcpyHostToDevice, (cudaStream_t)stream) ==
+                 cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
+}
+
+int acs_engine_run(acs_engine* e, int32_t steps, int32_t record_every, int32_t record_last, void* stream) {
+  if (!e || steps < 1 || record_every < 0) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<char> rec_at(steps, 0);
+  int nrec = 0;
+  for (int k = 0; k < steps; ++k) {
+    rec_at[k] = (record_every > 0 && (k + 1) % record_every == 0) || (record_last && k == steps - 1);
+    nrec += rec_at[k];
+  }
+  if (nrec > e->E.rec_cap) return ACS_ERR_ARG;
+  long long key = ((long long)steps << 32) ^ ((long long)record_every << 1) ^ (record_last ? 1 : 0);
+  auto it = e->graphs.find(key);
+  cudaGraphExec_t exec = nullptr;
+  if (it == e->graphs.end()) {
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return ACS_ERR_CUDA;
+    cudaGraph_t g = nullptr;
+    int st = ACS_OK;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) st = ACS_ERR_CUDA;
+    if (!st) st = enqueue_block(e, steps, rec_at, cs);
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (st || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return st ? st : ACS_ERR_CUDA;
+    }
+    if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return ACS_ERR_CUDA;
+    }
+    cudaGraphDestroy(g);
+    if (e->graphs.size() > 16) {
+      for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+      e->graphs.clear();
+    }
+    e->graphs[key] = exec;
+  } else {
+    exec = it->second;
+  }
+  return cudaGraphLaunch(exec, s) == cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
+}
+
+int acs_engine_records(acs_engine* e, double* out, int32_t count, void* stream) {
+  if (!e || !out || count < 0 || count > e->E.rec_cap) return ACS_ERR_ARG;
+  if (count == 0) return ACS_OK;
+  return cudaMemcpyAsync(out, e->E.rec, 8 * (size_t)count * e->E.R * kRecW, cudaMemcpyDeviceToDevice,
+                         (cudaStream_t)stream) == cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
+}
+
+int acs_engine_status(acs_engine* e, acs_dev_status* out, int clear, void* stream) {
+  if (!e || !out) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(out, e->E.status, sizeof(acs_dev_status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return ACS_ERR_CUDA;
+  if (clear) {
+    acs_dev_status z{};
+    z.fail_step = -1;
+    z.rebuilds = out->rebuilds;
+    if (cudaMemcpyAsync(e->E.status, &z, sizeof(z), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return ACS_ERR_CUDA;
+  }
+  return ACS_OK;
+}
+
+int acs_engine_neighbor_stats(acs_engine* e, int32_t* max_nnb, int64_t* sum_nnb, void* stream) {
+  if (!e) return ACS_ERR_ARG;
+  std::vector<int32_t> h(e->E.S);
+  if (cudaMemcpyAsync(h.data(), e->E.nnb, 4 * (size_t)e->E.S, cudaMemcpyDeviceToHost, (cudaStream_t)stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return ACS_ERR_CUDA;
+  int32_t mx = 0;
+  int64_t sm = 0;
+  for (int32_t v : h) {
+    mx = std::max(mx, v);
+    sm += v;
+  }
+  if (max_nnb) *max_nnb = mx;
+  if (sum_nnb) *sum_nnb = sm;
+  return ACS_OK;
+}
+
+int acs_engine_launch_info(acs_engine* e, int32_t* step_blocks, int32_t* coop_blocks, int64_t* slots) {
+  if (!e) return ACS_ERR_ARG;
+  if (step_blocks) *step_blocks = e->step_blocks;
+  if (coop_blocks) *coop_blocks = e->coop_blocks;
+  if (slots) *slots = e->E.S;
+  return ACS_OK;
+}
+
+int acs_engine_load_state(acs_engine* e, const double* pos, const double* vel, void* stream) {
+  if (!e || !pos || !vel) return ACS_ERR_ARG;
+  k_load_keep<<<e->step_blocks, 256, 0, (cudaStream_t)stream>>>(e->E, pos, vel, e->src0_dev);
+  return launch_status();
+}
+
+int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* stream) {
+  if (!e || !out_dev) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(out_dev, 0, 16, s) != cudaSuccess) return ACS_ERR_CUDA;
+  // images of buffer 0 are current after acs_engine_set_state (and after any rebuild into buffer 0)
+  k_count_pairs<<<e->step_blocks, 256, 0, s>>>(e->E, e->ff, 0, out_dev);
+  return launch_status();
+}
+
+// The same launch sequence as one graph block, launched eagerly with CUDA events around every kernel, for
+// per-kernel timing. out_ms[0] = total step-kernel ms, [1] = total list-maintenance ms, [2] = step launches,
+// [3] = list-maintenance launches. Synchronous.
+int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, float* out_ms, void* stream) {
+  if (!e || steps < 1 || !out_ms) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<cudaEvent_t> ev(4 * (size_t)steps + 4);
+  for (auto& x : ev)
+    if (cudaEventCreate(&x) != cudaSuccess) return ACS_ERR_CUDA;
+  int st = ACS_OK;
+  size_t ne = 0;
+  std::vector<std::pair<size_t, int>> spans;  // (first event index, kind)
+  auto mark = [&](int kind, auto&& launch) {
+    cudaEventRecord(ev[ne], s);
+    int r = launch();
+    cudaEventRecord(ev[ne + 1], s);
+    spans.push_back({ne, kind});
+    ne += 2;
+    return r;
+  };
+  k_prologue<<<e->step_blocks, 256, 0, s>>>(e->E, 0);
+  st = launch_status();
+  if (!st) st = launch_rebuild(e, 0, 0, 0, 0, s);
+  int rec_idx = 0;
+  for (int k = 0; k < steps && !st; ++k) {
+    const int src = k & 1, dst = (k + 1) & 1;
+    const bool last = (k == steps - 1);
+    const int rec = ((record_every > 0 && (k + 1) % record_every == 0) || last) ? 1 : 0;
+    st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, s); });
+    if (!st) st = mark(1, [&] { return launch_rebuild(e, dst, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, 0, s); });
+    rec_idx += rec;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) st = ACS_ERR_CUDA;
+  float tot[2] = {0.f, 0.f};
+  int cnt[2] = {0, 0};
+  for (auto& sp : spans) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev[sp.first], ev[sp.first + 1]) == cudaSuccess) {
+      tot[sp.second] += ms;
+      cnt[sp.second] += 1;
+    }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  out_ms[0] = tot[0];
+  out_ms[1] = tot[1];
+  out_ms[2] = (float)cnt[0];
+  out_ms[3] = (float)cnt[1];
+  return st;
+}
+
+int acs_engine_destroy(acs_engine* e) {
+  if (!e) return ACS_OK;
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  delete e;
+  return ACS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,449 @@
+"""Host side of the device-resident engine (include/accusim_b200_engine.h).
+
+`GpuSimulation` runs `Simulation.run(duration, steps, record_every, positions)` of accusim
+(accusim/simulation.py:95-112) with VelocityVerlet and LennardJones and/or DampedShiftedCoulomb as
+CUDA-graph-captured step loops: FP32 pair terms with Kahan-compensated per-atom sums, FP64 positions,
+velocities, integration and conserved-quantity sums. `Engine` is the thin ctypes wrapper; it also
+advances batches of independent replicas (see `ensemble.py`).
+
+Engine units: length A, mass u, energy kJ/mol per particle, charge e (time unit ~0.1 ps). The SI
+conversion happens here, at the API edge; results are returned in SI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import require_cuda, stream_handle, to_dev
+from .units import N_A, amu, e_charge, k_e
+
+LEN = 1e-10
+MASS = amu
+ENERGY = 1e3 / N_A
+TIME = LEN * math.sqrt(MASS / ENERGY)
+VEL = LEN / TIME
+ACC = VEL / TIME
+CHARGE = e_charge
+KE_ENGINE = k_e * CHARGE ** 2 / (ENERGY * LEN)
+
+P = C.c_void_p
+
+
+class Replica(C.Structure):
+    _fields_ = [("n", C.c_int32), ("pad", C.c_int32), ("box", C.c_double * 3), ("dt", C.c_double),
+                ("rlist", C.c_double), ("half_skin", C.c_double)]
+
+
+class ForceField(C.Structure):
+    _fields_ = [("n_species", C.c_int32), ("lj", C.c_int32), ("dsf", C.c_int32), ("pad", C.c_int32),
+                ("mass", C.c_double * 8), ("lj_eps", C.c_double * 64), ("lj_sig", C.c_double * 64),
+                ("lj_cutoff", C.c_double), ("dsf_alpha", C.c_double), ("dsf_rcut", C.c_double),
+                ("dsf_k", C.c_double), ("q", C.c_double * 8)]
+
+
+class EngineConfig(C.Structure):
+    _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
+                ("replicas", C.POINTER(Replica)), ("ff", ForceField)]
+
+
+class DevStatusC(C.Structure):
+    _fields_ = [("flags", C.c_int32), ("need_nbr", C.c_int32), ("rebuilds", C.c_int32), ("fail_step", C.c_int32),
+                ("steps_done", C.c_int32), ("pad", C.c_int32 * 3)]
+
+
+ENGINE_SIGNATURES = {
+    "acs_engine_bytes": (C.c_size_t, [C.POINTER(EngineConfig)]),
+    "acs_engine_create": (C.c_int, [C.POINTER(EngineConfig), P, C.c_size_t, C.POINTER(P)]),
+    "acs_engine_set_state": (C.c_int, [P, P, P, P, P]),
+    "acs_engine_get_state": (C.c_int, [P, P, P, P, P]),
+    "acs_engine_set_active": (C.c_int, [P, P, P]),
+    "acs_engine_run": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P]),
+    "acs_engine_records": (C.c_int, [P, P, C.c_int32, P]),
+    "acs_engine_status": (C.c_int, [P, C.POINTER(DevStatusC), C.c_int, P]),
+    "acs_engine_neighbor_stats": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), P]),
+    "acs_engine_launch_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "acs_engine_load_state": (C.c_int, [P, P, P, P]),
+    "acs_engine_count_pairs": (C.c_int, [P, P, P]),
+    "acs_engine_run_timed": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(C.c_float), P]),
+    "acs_engine_destroy": (C.c_int, [P]),
+}
+_lib.SIGNATURES.update(ENGINE_SIGNATURES)
+
+REC_FIELDS = ("KE", "PE", "Px", "Py", "Pz", "Lx", "Ly", "Lz")
+
+
+def forcefield_from(forces, species) -> tuple[ForceField, float, float]:
+    """Engine force field from reference-shaped LennardJones / DampedShiftedCoulomb objects (SI).
+    Returns (ff, list radius [m], half skin [m]) for the combined neighbour list: every pair within any
+    force's cutoff stays listed until an atom has moved half of the smallest effective skin."""
+    ff = ForceField()
+    ns = len(species)
+    if ns > 8:
+        raise ValueError("the engine supports up to 8 species")
+    ff.n_species = ns
+    for a, sp in enumerate(species):
+        ff.mass[a] = sp.mass / MASS
+        ff.q[a] = sp.charge / CHARGE
+    radii = []   # (cutoff_max, list radius) per force, SI
+    lj = [f for f in forces if type(f).__name__ == "LennardJones"]
+    dsf = [f for f in forces if type(f).__name__ == "DampedShiftedCoulomb"]
+    if len(lj) + len(dsf) != len(forces) or len(lj) > 1 or len(dsf) > 1 or not forces:
+        raise ValueError("the engine runs one LennardJones and/or one DampedShiftedCoulomb force")
+    if lj:
+        f = lj[0]
+        eps, sig = f._tables(_SpeciesView(species))
+        if not np.any(eps > 0):
+            raise ValueError("LennardJones has no interacting species")
+        ff.lj = 1
+        ff.lj_cutoff = float(f.cutoff)
+        for a in range(ns):
+            for b in range(ns):
+                ff.lj_eps[a * ns + b] = eps[a, b] / ENERGY
+                ff.lj_sig[a * ns + b] = sig[a, b] / LEN
+        smax = float(np.max(np.where(eps > 0, sig, 0)))
+        radii.append((f.cutoff * smax, f.cutoff * smax + f.skin * smax))
+    if dsf:
+        f = dsf[0]
+        if f.exclude:
+            raise ValueError("the engine does not take DSF exclusions; use the drop-in plug-ins")
+        ff.dsf = 1
+        ff.dsf_alpha = f.alpha * LEN
+        ff.dsf_rcut = f.rcut / LEN
+        ff.dsf_k = f.k * CHARGE ** 2 / (ENERGY * LEN)
+        radii.append((f.rcut, f.rcut + f.skin))
+    rlist = max(r for _, r in radii)
+    half_skin = 0.5 * min(rlist - c for c, _ in radii)
+    return ff, rlist, half_skin
+
+
+class _SpeciesView:
+    def __init__(self, species):
+        self.species = species
+
+
+class Engine:
+    """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
+
+    def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0):
+        require_cuda()
+        L = _lib.lib()
+        for name, (res, args) in ENGINE_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        self.L = L
+        self.R = len(replicas)
+        self._reps = (Replica * self.R)()
+        for k, r in enumerate(replicas):
+            self._reps[k].n = int(r["n"])
+            for d in range(3):
+                self._reps[k].box[d] = float(r["box"][d])
+            self._reps[k].dt = float(r["dt"])
+            self._reps[k].rlist = float(r["rlist"])
+            self._reps[k].half_skin = float(r["half_skin"])
+        self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self._reps, ff)
+        nbytes = L.acs_engine_bytes(C.byref(self.cfg))
+        if nbytes == 0:
+            raise ValueError("engine configuration rejected (sizes, list radius >= box/2, or too many replicas)")
+        self.nbytes = int(nbytes)
+        self.mem = torch.empty(self.nbytes + 256, dtype=torch.uint8, device="cuda")
+        base = self.mem.data_ptr()
+        off = (-base) % 256
+        self.h = P()
+        _lib.check(L.acs_engine_create(C.byref(self.cfg), base + off, self.nbytes, C.byref(self.h)),
+                   "acs_engine_create")
+        self.maxnb = int(maxnb)
+        self.rec_cap = int(rec_cap)
+        self.counts = np.array([int(r["n"]) for r in replicas])
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)])
+        self._rec_buf = torch.empty(rec_cap * self.R * 8, dtype=torch.float64, device="cuda")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                self.L.acs_engine_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def set_state(self, pos_d, vel_d, sp_d):
+        _lib.check(self.L.acs_engine_set_state(self.h, pos_d.data_ptr(), vel_d.data_ptr(), sp_d.data_ptr(),
+                                               stream_handle()), "acs_engine_set_state")
+
+    def load_state(self, pos_d, vel_d):
+        """Positions/velocities in caller order (engine units) replacing the current ones; lists kept."""
+        _lib.check(self.L.acs_engine_load_state(self.h, pos_d.data_ptr(), vel_d.data_ptr(), stream_handle()),
+                   "acs_engine_load_state")
+
+    def count_pairs(self):
+        """(LJ, DSF) unique pairs inside the physical cutoffs, counted on the device."""
+        out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        _lib.check(self.L.acs_engine_count_pairs(self.h, out.data_ptr(), stream_handle()), "acs_engine_count_pairs")
+        a, b = out.cpu().numpy()
+        return int(a) // 2, int(b) // 2
+
+    def get_state(self):
+        n = int(self.offsets[-1])
+        pos = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        vel = torch.empty_like(pos)
+        acc = torch.empty_like(pos)
+        _lib.check(self.L.acs_engine_get_state(self.h, pos.data_ptr(), vel.data_ptr(), acc.data_ptr(),
+                                               stream_handle()), "acs_engine_get_state")
+        return pos, vel, acc
+
+    def set_active(self, active):
+        a = np.ascontiguousarray(np.asarray(active, dtype=np.int32))
+        _lib.check(self.L.acs_engine_set_active(self.h, a.ctypes.data, stream_handle()), "acs_engine_set_active")
+        torch.cuda.current_stream().synchronize()
+
+    def run(self, steps: int, record_every: int = 0, record_last: bool = True):
+        _lib.check(self.L.acs_engine_run(self.h, int(steps), int(record_every), 1 if record_last else 0,
+                                         stream_handle()), "acs_engine_run")
+
+    def run_timed(self, steps: int, record_every: int = 0):
+        """Eager launches of one block with per-kernel CUDA events: (step ms avg, rebuild ms avg, total ms)."""
+        out = (C.c_float * 4)()
+        _lib.check(self.L.acs_engine_run_timed(self.h, int(steps), int(record_every), out, stream_handle()),
+                   "acs_engine_run_timed")
+        return out[0] / max(out[2], 1), out[1] / max(out[3], 1), out[0] + out[1]
+
+    def records(self, count: int) -> np.ndarray:
+        """(count, R, 8) FP64 records [KE, PE, Px, Py, Pz, Lx, Ly, Lz] in engine units."""
+        if count == 0:
+            return np.zeros((0, self.R, 8))
+        _lib.check(self.L.acs_engine_records(self.h, self._rec_buf.data_ptr(), int(count), stream_handle()),
+                   "acs_engine_records")
+        return self._rec_buf[: count * self.R * 8].view(count, self.R, 8).cpu().numpy()
+
+    def status(self, clear=False) -> DevStatusC:
+        st = DevStatusC()
+        _lib.check(self.L.acs_engine_status(self.h, C.byref(st), 1 if clear else 0, stream_handle()),
+                   "acs_engine_status")
+        return st
+
+    def check(self, where="engine"):
+        st = self.status()
+        if st.flags & _lib.FLAG_OVERFLOW:
+            raise _lib.ListOverflow(_lib.ACS_ERR_LIST_OVERFLOW, f"{where}: need {st.need_nbr} neighbours")
+        if st.flags & _lib.FLAG_NONFINITE:
+            raise _lib.AcsError(_lib.ACS_ERR_NONFINITE, where)
+        if st.flags & _lib.FLAG_TIMEOUT:
+            raise _lib.AcsError(_lib.ACS_ERR_TIMEOUT, where)
+        return st
+
+    def neighbor_stats(self):
+        mx, sm = C.c_int32(), C.c_int64()
+        _lib.check(self.L.acs_engine_neighbor_stats(self.h, C.byref(mx), C.byref(sm), stream_handle()))
+        return mx.value, sm.value
+
+    def launch_info(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int64()
+        _lib.check(self.L.acs_engine_launch_info(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+
+def estimate_maxnb(n, box, rlist):
+    rho = n / float(np.prod(box))
+    expected = rho * 4.0 / 3.0 * math.pi * rlist ** 3
+    return int(min(expected * 1.3 + 32, 4096) + 7) // 8 * 8
+
+
+def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0):
+    """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
+    (engine, rlist, half_skin) with the radii in SI."""
+    ff, rlist, half_skin = forcefield_from(forces, species)
+    reps = [dict(n=r["n"], box=np.asarray(r["box"], float) / LEN, dt=r["dt"] / TIME, rlist=rlist / LEN,
+                 half_skin=half_skin / LEN) for r in replicas_si]
+    if maxnb is None:
+        maxnb = max(estimate_maxnb(r["n"], r["box"], r["rlist"]) for r in reps)
+    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult), rlist, half_skin
+
+
+def _upload_state(engine, systems):
+    ns = len(systems[0].species)
+    for s in systems:
+        if s.n and (s.sp.min() < 0 or s.sp.max() >= ns):
+            raise ValueError("species index out of range")
+        if not np.all(np.isfinite(s.pos)) or not np.all(np.isfinite(s.vel)):
+            raise ValueError("non-finite positions or velocities")
+    pos = np.concatenate([s.pos for s in systems]) / LEN
+    vel = np.concatenate([s.vel for s in systems]) / VEL
+    sp = np.concatenate([s.sp for s in systems]).astype(np.int32)
+    engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
+
+
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0):
+    """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
+    grows the neighbour capacity once if the first build overflows."""
+    for s in systems:
+        if s.dim != 3 or not s.periodic:
+            raise ValueError("the engine runs 3-dimensional periodic systems")
+    species = systems[0].species
+    reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
+    for attempt in range(3):
+        eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult)
+        _upload_state(eng, systems)
+        st = eng.status()
+        if st.flags & _lib.FLAG_OVERFLOW:
+            maxnb = int(st.need_nbr * 1.2 + 16 + 7) // 8 * 8
+            continue
+        eng.check("engine start")
+        mx, _ = eng.neighbor_stats()
+        if mx * 1.15 + 8 > eng.maxnb and attempt == 0 and maxnb is None:
+            maxnb = int(mx * 1.3 + 16 + 7) // 8 * 8
+            continue
+        return eng, rlist, hs
+    raise _lib.ListOverflow(_lib.ACS_ERR_LIST_OVERFLOW, "engine start")
+
+
+class GpuSimulation:
+    """`Simulation` with the step loop on the device (accusim/simulation.py:40-131 interface).
+
+    forces: [LennardJones] and/or [DampedShiftedCoulomb] (this package's or the reference's classes);
+    integrator: VelocityVerlet only. `system.pos`/`vel` are synchronised from the device after every
+    `run` call (and at records when positions=True)."""
+
+    def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
+                 rec_cap=256, grid_mult=0):
+        from .integrators import VelocityVerlet
+        from .simulation import Trajectory
+        from .units import si
+        if reactions:
+            raise NotImplementedError("reactions are not part of the accusim_b200 force-and-step path")
+        if integrator is not None and type(integrator).__name__ != "VelocityVerlet":
+            raise ValueError("GpuSimulation integrates with VelocityVerlet")
+        self.system = system
+        self.forces = list(forces)
+        self.integrator = integrator or VelocityVerlet()
+        self.dt = None if dt is None else si(dt, "s")
+        self.seed = seed
+        self.rng = np.random.default_rng(seed)
+        self.reactions = None
+        self.time = 0.0
+        self.steps = 0
+        self.trajectory = Trajectory()
+        self._initial = None
+        self.engine, self.rlist, self.half_skin = start_engine(
+            [system], self.forces, [self.dt if self.dt is not None else 1e-15], maxnb=maxnb, rec_cap=rec_cap,
+            grid_mult=grid_mult)
+        self._last = self.engine.records(1)[0, 0]
+        self._pull()
+
+    # state ------------------------------------------------------------------------------------------
+    def _pull(self):
+        pos, vel, acc = self.engine.get_state()
+        s = self.system
+        s.pos = pos.cpu().numpy() * LEN
+        s.vel = vel.cpu().numpy() * VEL
+        self.acc = acc.cpu().numpy() * ACC
+        self.force = self.acc * s.masses[:, None]
+        self.pe = float(self._last[1] * ENERGY)
+
+    @property
+    def rebuilds(self):
+        return int(self.engine.status().rebuilds)
+
+    def _record(self, rec, positions):
+        s, tr = self.system, self.trajectory
+        tr.t.append(self.time)
+        tr.kinetic.append(float(rec[0] * ENERGY))
+        tr.potential.append(float(rec[1] * ENERGY))
+        tr.internal.append(float(np.sum(s.eint)))
+        tr.released.append(0.0)
+        tr.momentum.append(rec[2:5] * (MASS * VEL))
+        tr.angular_momentum.append(rec[5:8] * (MASS * VEL * LEN))
+        tr.mass.append(float(np.sum(s.masses)))
+        tr.charge.append(float(np.sum(s.charges)))
+        tr.counts.append(s.counts())
+        tr.bath.append(0.0)
+        if positions:
+            tr.positions.append(s.pos.copy())
+            tr.velocities.append(s.vel.copy())
+            tr.species.append(s.sp.copy())
+
+    def run(self, duration=None, steps=None, record_every=1, positions=True):
+        """Advance `steps` VelocityVerlet steps; record after every `record_every`-th step and the last
+        (accusim/simulation.py:95-112). Blocks of steps run as one cached CUDA graph each; a block ends at
+        every record when positions are recorded (they come back to the host there)."""
+        from .units import si
+        if self.dt is None:
+            raise ValueError("set dt (or use accusim.advisor.suggest_dt)")
+        if steps is None:
+            steps = int(round(si(duration, "s") / self.dt))
+        re = max(int(record_every), 1)
+        if not self.trajectory.t:
+            if self._initial is None:
+                self._initial = _InitialState(self.system.copy(), self)
+            self._record(self._last, positions)
+        eng = self.engine
+        done = 0
+        while done < steps:
+            left = steps - done
+            if positions:
+                block = min(re, left)
+            else:
+                span = re * max(1, min(eng.rec_cap - 1, 4000 // re))
+                block = min(span, left)
+            end_of_run = block == left
+            periodic = 0 if positions else re
+            eng.run(block, periodic, end_of_run or positions)
+            marks = [] if positions else list(range(re, block + 1, re))
+            if (end_of_run or positions) and (not marks or marks[-1] != block):
+                marks.append(block)
+            recs = eng.records(len(marks))[:, 0, :]
+            eng.check("engine run")
+            if positions:
+                self._pull_positions()
+            j0 = 0
+            for j, rec in zip(marks, recs):
+                for _ in range(j - j0):
+                    self.time += self.dt
+                j0 = j
+                self._record(rec, positions)
+            for _ in range(block - j0):
+                self.time += self.dt
+            self._last = recs[-1]
+            self.steps += block
+            done += block
+        self._pull()
+        return self.trajectory
+
+    def _pull_positions(self):
+        pos, vel, _ = self.engine.get_state()
+        self.system.pos = pos.cpu().numpy() * LEN
+        self.system.vel = vel.cpu().numpy() * VEL
+
+    def update_forces(self):
+        """Re-evaluate forces of the current host state on the device (after host-side edits)."""
+        _upload_state(self.engine, [self.system])
+        self.engine.check("update_forces")
+        self._last = self.engine.records(1)[0, 0]
+        self._pull()
+
+    def clone(self, dt=None):
+        sim = GpuSimulation(self.system.copy(), self.forces, integrator=self.integrator,
+                            dt=self.dt if dt is None else dt, seed=self.seed, maxnb=self.engine.maxnb,
+                            rec_cap=self.engine.rec_cap)
+        return sim
+
+    def accuracy_report(self, convergence_duration=None):
+        from .accuracy import AccuracyReport
+        return AccuracyReport.build(self, convergence_duration)
+
+
+class _InitialState:
+    """Start state of a GpuSimulation run, kept on the host; `clone(dt)` makes a fresh simulation from it
+    (the role of `Simulation._initial` in accusim/simulation.py:101-102 and accuracy.py:200-205)."""
+
+    def __init__(self, system, sim):
+        self.system = system
+        self._sim = sim
+
+    def clone(self, dt=None):
+        s = self._sim
+        return GpuSimulation(self.system.copy(), s.forces, integrator=s.integrator, dt=s.dt if dt is None else dt,
+                             seed=s.seed, maxnb=s.engine.maxnb, rec_cap=s.engine.rec_cap)

@@ -1,0 +1,87 @@
+/*
+ * accusim_b200 engine: device-resident fast path for Simulation.run with VelocityVerlet and
+ * LennardJones and/or DampedShiftedCoulomb (accusim/simulation.py:95-112, integrators.py:25-31,
+ * forces.py:78-175, :391-452), for one periodic system or a batch of independent replicas.
+ *
+ * Arithmetic: FP64 positions (as offsets from cell origins) and velocities, FP64 integration and
+ * conserved-quantity sums; FP32 pair terms with Kahan-compensated per-atom force and energy sums.
+ * Units are the caller's (the Python layer uses A, u, kJ/mol, e). Memory: the caller allocates one
+ * 256-byte-aligned device block of acs_engine_bytes() and passes it to acs_engine_create; the engine
+ * keeps only host-side bookkeeping and cached CUDA graphs. Multi-step runs are CUDA graphs of
+ * one fused force/kick/drift kernel and one cooperative list-maintenance kernel per step.
+ */
+#ifndef ACCUSIM_B200_ENGINE_H
+#define ACCUSIM_B200_ENGINE_H
+
+#include "accusim_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct acs_replica {
+  int32_t n;          /* atoms */
+  int32_t pad;
+  double box[3];      /* periodic box edges */
+  double dt;          /* time step */
+  double rlist;       /* neighbour-list radius = largest cutoff + skin (must be < box/2) */
+  double half_skin;   /* rebuild once an atom has moved this far since the last build */
+} acs_replica;
+
+typedef struct acs_forcefield {
+  int32_t n_species;  /* <= 8 */
+  int32_t lj;         /* LennardJones term on */
+  int32_t dsf;        /* DampedShiftedCoulomb term on */
+  int32_t pad;
+  double mass[8];
+  double lj_eps[64];  /* n_species x n_species, mixed (Lorentz-Berthelot) */
+  double lj_sig[64];
+  double lj_cutoff;   /* in units of sigma_ij; energy shifted to zero there */
+  double dsf_alpha, dsf_rcut, dsf_k;
+  double q[8];        /* charge per species */
+} acs_forcefield;
+
+typedef struct acs_engine_config {
+  int32_t n_replicas;
+  int32_t maxnb;      /* neighbour capacity per atom */
+  int32_t rec_cap;    /* records kept per run call */
+  int32_t grid_mult;  /* step kernel: blocks per SM (0 = one thread per atom slot) */
+  const acs_replica* replicas;  /* host array */
+  acs_forcefield ff;
+} acs_engine_config;
+
+typedef struct acs_engine acs_engine;
+
+size_t acs_engine_bytes(const acs_engine_config* cfg);
+int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs_engine** out);
+/* pos/vel: device, replica-concatenated (n_r x 3 each, caller units), species: device int32.
+ * Builds every list, evaluates forces, and writes the initial records at index 0. */
+int acs_engine_set_state(acs_engine* e, const double* pos, const double* vel, const int32_t* species, void* stream);
+/* Device outputs in caller order; positions wrapped into [0, box) as accusim/system.py:127 does. */
+int acs_engine_get_state(acs_engine* e, double* pos, double* vel, double* acc, void* stream);
+/* Host array of n_replicas flags: inactive replicas are skipped by later runs. */
+int acs_engine_set_active(acs_engine* e, const int32_t* active_host, void* stream);
+/* Advance active replicas by `steps` (one cached CUDA graph per (steps, record schedule)). Records are
+ * taken after steps k with (k+1) % record_every == 0 and, if record_last, after the last step; record i
+ * of replica r is [KE, PE, Px, Py, Pz, Lx, Ly, Lz] at rec[(i * n_replicas + r) * 8]. */
+int acs_engine_run(acs_engine* e, int32_t steps, int32_t record_every, int32_t record_last, void* stream);
+int acs_engine_records(acs_engine* e, double* out_dev, int32_t count, void* stream);
+/* Replace positions/velocities (device, caller order, wrapped or not) keeping the current lists and
+ * accelerations; the next run's skin test rebuilds the lists if the new positions require it. */
+int acs_engine_load_state(acs_engine* e, const double* pos, const double* vel, void* stream);
+/* out_dev[0] = ordered LJ pairs inside cutoff*sigma_ij, out_dev[1] = ordered DSF pairs inside rc (each
+ * unordered pair counted twice), on the images set by the last acs_engine_set_state. */
+int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* stream);
+/* Synchronous: copies the device status block to *out (optionally clearing its error flags). */
+int acs_engine_status(acs_engine* e, acs_dev_status* out, int clear, void* stream);
+int acs_engine_neighbor_stats(acs_engine* e, int32_t* max_nnb, int64_t* sum_nnb, void* stream);
+int acs_engine_launch_info(acs_engine* e, int32_t* step_blocks, int32_t* coop_blocks, int64_t* slots);
+/* The launch sequence of one block, eager, with CUDA events around every kernel (synchronous):
+ * out_ms = {step-kernel ms total, list-maintenance ms total, step launches, list-maintenance launches}. */
+int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, float* out_ms, void* stream);
+int acs_engine_destroy(acs_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACCUSIM_B200_ENGINE_H */

@@ -1,0 +1,143 @@
+"""Device-resident engine (FP32-compensated pairs, FP64 integration) against the FP64 oracle and the
+reference's golden vectors. Floating-point tolerances (FP32 pair arithmetic):
+  force RMS error / force RMS   <= 2e-6   (LJ),  <= 5e-6 (LJ + DSF)
+  potential energy relative     <= 2e-6
+  records vs host FP64 sums of the downloaded state: 1e-12 relative (same FP64 data)
+  momentum drift (report metric max|P-P0| / sum m|v|) <= 1e-9 (the report's PASS grade)."""
+import numpy as np
+import pytest
+
+from oracle import accusim_port as port
+from tests._helpers import rel_max
+from tests.test_dropin_gpu import product_system
+
+pytestmark = pytest.mark.gpu
+
+
+def rms_rel(F, Fref):
+    return float(np.sqrt(np.mean(np.sum((F - Fref) ** 2, 1)) / np.mean(np.sum(Fref ** 2, 1))))
+
+
+def oracle_of(s):
+    return port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                      [(x.name, x.mass, x.charge) for x in s.species])
+
+
+def test_engine_lj_forces_fp32c_vs_oracle(golden):
+    from devinproj_b200 import GpuSimulation, LennardJones
+    g = golden("argon864")
+    s = product_system(g)
+    params = {"Ar": (float(g["eps"]), float(g["sig"]))}
+    sim = GpuSimulation(s, [LennardJones(params, cutoff=2.5)], dt=float(g["dt"]))
+    Fo, Uo = port.LennardJones(params, cutoff=2.5, skin=0.0).compute(oracle_of(s))
+    e = rms_rel(sim.force, Fo)
+    print(f"argon864 FP32c force RMS rel error {e:.2e}, energy rel error {abs(sim.pe - Uo) / abs(Uo):.2e}")
+    assert e <= 2e-6
+    assert abs(sim.pe - Uo) <= 2e-6 * abs(Uo)
+    # exact antisymmetry: the net force is round-off of the per-atom sums only
+    assert np.linalg.norm(sim.force.sum(0)) <= 1e-6 * np.sqrt(s.n) * np.sqrt(np.mean(np.sum(Fo ** 2, 1)))
+
+
+def test_engine_nacl_lj_dsf_forces_vs_reference(golden):
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones
+    g = golden("nacl4096")
+    s = product_system(g)
+    params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+    forces = [LennardJones(params, cutoff=2.5), DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"]))]
+    sim = GpuSimulation(s, forces, dt=float(g["dt"]))
+    Fref = g["F_lj"] + g["F_dsf"]
+    Uref = float(g["U_lj"] + g["U_dsf"])
+    e = rms_rel(sim.force, Fref)
+    print(f"nacl4096 FP32c force RMS rel error {e:.2e}, energy rel error {abs(sim.pe - Uref) / abs(Uref):.2e}")
+    assert e <= 5e-6
+    assert abs(sim.pe - Uref) <= 2e-6 * abs(Uref)
+
+
+def test_engine_trajectory_tracks_reference_and_conserves(golden):
+    """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
+    from devinproj_b200 import GpuSimulation, LennardJones
+    from devinproj_b200.accuracy import energy_drift, momentum_drift
+    g = golden("argon864")
+    s = product_system(g, "0")
+    sim = GpuSimulation(s, [LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)],
+                        dt=float(g["dt"]))
+    tr = sim.run(steps=int(g["steps"]), positions=False)
+    E = np.array(tr.kinetic) + np.array(tr.potential)
+    Eref = g["kinetic"] + g["potential"]
+    scale = max(abs(Eref[0]), np.max(np.abs(g["kinetic"])), np.max(np.abs(g["potential"])))
+    assert np.max(np.abs(E - Eref)) <= 1e-5 * scale
+    assert rel_max(np.array(tr.kinetic), g["kinetic"]) <= 1e-4
+    assert momentum_drift(tr, s) <= 1e-9
+    ref_drift = port.energy_drift(Eref, g["kinetic"], g["potential"])
+    assert energy_drift(tr) <= 1.5 * ref_drift + 1e-6
+    assert len(tr.t) == int(g["steps"]) + 1 and tr.t[-1] == pytest.approx(float(g["dt"]) * int(g["steps"]))
+
+
+def test_engine_records_equal_host_sums_of_state():
+    from devinproj_b200 import GpuSimulation, configs
+    s, forces, dt = configs.argon864(seed=4)
+    sim = GpuSimulation(s, forces, dt=dt)
+    tr = sim.run(steps=37, record_every=10, positions=True)
+    assert len(tr.t) == 1 + 3 + 1
+    assert len(tr.positions) == len(tr.t)
+    assert np.array_equal(tr.positions[-1], s.pos)
+    assert tr.kinetic[-1] == pytest.approx(s.kinetic_energy(), rel=1e-12)
+    assert np.allclose(tr.momentum[-1], s.momentum(), rtol=0, atol=1e-12 * np.sum(s.masses[:, None] * np.abs(s.vel)))
+    L = s.angular_momentum()
+    assert np.allclose(tr.angular_momentum[-1], L, rtol=1e-10, atol=1e-12 * np.abs(L).max())
+    assert np.all(s.pos >= 0) and np.all(s.pos < s.box)
+
+
+def test_engine_lists_stay_valid_across_rebuilds():
+    """Hot argon: many rebuilds and re-sorts; forces at the end equal the FP64 oracle's on the same state."""
+    from devinproj_b200 import GpuSimulation, configs
+    s, forces, dt = configs.argon864(seed=1)
+    s.maxwell_boltzmann(300.0, np.random.default_rng(1))
+    sim = GpuSimulation(s, forces, dt=dt)
+    sim.run(steps=300, record_every=100, positions=False)
+    assert sim.rebuilds >= 10
+    Fo, Uo = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(oracle_of(s))
+    assert rms_rel(sim.force, Fo) <= 2e-6
+    assert abs(sim.pe - Uo) <= 2e-6 * abs(Uo)
+
+
+def test_batched_replicas_equal_single_runs_bitwise():
+    """Replicas of different sizes and dt in one engine advance exactly as each would alone."""
+    from devinproj_b200 import configs
+    from devinproj_b200.engine import LEN, VEL, start_engine
+    systems, dts = [], []
+    for nc, T, dtf in [(4, 0.72, 1.0), (5, 1.0, 0.5), (6, 0.72, 0.25)]:
+        s, lj = configs.lj_fluid(nc, T_star=T, seed=nc)
+        systems.append(s)
+        dts.append(0.005 * configs.AR_TAU * dtf)
+    batch, _, _ = start_engine(systems, [lj], dts)
+    batch.run(50, 0, True)
+    bp, bv, _ = batch.get_state()
+    bp, bv = bp.cpu().numpy(), bv.cpu().numpy()
+    for k, (s, dt) in enumerate(zip(systems, dts)):
+        eng, _, _ = start_engine([s], [lj], [dt], maxnb=batch.maxnb)
+        eng.run(50, 0, True)
+        p, v, _ = eng.get_state()
+        sl = slice(batch.offsets[k], batch.offsets[k + 1])
+        assert np.array_equal(p.cpu().numpy(), bp[sl])
+        assert np.array_equal(v.cpu().numpy(), bv[sl])
+    assert batch.status().rebuilds > 3
+
+
+def test_engine_rejects_unsupported_setups():
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones, System
+    s = System(3, box=None)
+    s.add_species("Ar", 6.6e-26)
+    s.add("Ar", np.random.default_rng(0).uniform(0, 3e-9, (50, 3)))
+    with pytest.raises(ValueError):
+        GpuSimulation(s, [LennardJones({"Ar": (1.6e-21, 3.4e-10)})], dt=1e-15)
+    s2 = System(3, box=4e-10, periodic=True)   # list radius >= box/2
+    s2.add_species("Ar", 6.6e-26)
+    s2.add("Ar", [[0, 0, 0], [2e-10, 0, 0]])
+    with pytest.raises(ValueError):
+        GpuSimulation(s2, [LennardJones({"Ar": (1.6e-21, 3.4e-10)})], dt=1e-15)
+    s3 = System(3, box=4e-9, periodic=True)
+    s3.add_species("Na", 3.8e-26, charge=1.6e-19)
+    s3.add("Na", [[0, 0, 0], [2e-10, 0, 0]])
+    with pytest.raises(ValueError):
+        GpuSimulation(s3, [DampedShiftedCoulomb(rcut=1e-9, exclude=[(0, 1)])], dt=1e-15)
