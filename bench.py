@@ -187,6 +187,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--record-every", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tpa", type=int, default=None, help="threads per atom in the pair kernel (default: auto)")
+    ap.add_argument("--profile", action="store_true",
+                    help="engine only: warm-up graph steps then --steps eager launches (for ncu), no timing legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -212,12 +215,25 @@ def main():
     from devinproj_b200.engine import ACC, LEN, VEL, start_engine
 
     s, forces, dt, cfg = workload(args.workload, seed=rank)
-    eng, rlist, hs = start_engine([s], forces, [dt], rec_cap=max(args.steps // args.record_every + 2, 4))
+    eng, rlist, hs = start_engine([s], forces, [dt], rec_cap=max(args.steps // args.record_every + 2, 4), tpa=args.tpa)
     n = s.n
     pairs_lj, pairs_dsf = eng.count_pairs()
     step_blocks, coop_blocks, slots = eng.launch_info()
     init = eng.records(1)[0, 0].copy()
     stream = torch.cuda.current_stream()
+    if args.profile:
+        eng.run(args.warmup, 0, True)
+        torch.cuda.synchronize()
+        rb0 = eng.status().rebuilds
+        eng.phase_times(clear=True)
+        k_ms, r_ms, tot = eng.run_timed(args.steps, 0)
+        eng.check("profile")
+        nreb = eng.status().rebuilds - rb0
+        ph = {k: round(v / max(nreb, 1), 4) for k, v in eng.phase_times().items()}
+        print(json.dumps({"profile": cfg["workload"], "tpa": eng.tpa, "step_kernel_ms": k_ms, "list_kernel_ms": r_ms,
+                          "rebuilds": nreb, "ms_per_rebuild_by_phase": ph, "pairs_lj": pairs_lj,
+                          "pairs_dsf": pairs_dsf, "maxnb": eng.maxnb, "neighbors": eng.neighbor_stats()}))
+        return
 
     # warm-up (also instantiates the timed graph's sibling shapes)
     eng.run(args.warmup, 0, True)

@@ -33,7 +33,8 @@ namespace {
 
 constexpr int kMaxRep = 8192;   // replicas per engine (flag bitmap in shared memory)
 constexpr int kRecW = 8;        // KE, PE, Px, Py, Pz, Lx, Ly, Lz
-constexpr int kChunkTiles = 64; // record-reduction chunk, in 32-atom tiles
+constexpr int kChunkTiles = 64; // record-reduction chunk, in atom groups (G atoms each)
+constexpr int kCellChunk = 1024;  // cell-scan chunk (4 cells per thread of a 256-thread block)
 constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr long long kSpinLimit = 20000000;  // ~2 s of 100 ns sleeps
@@ -44,7 +45,8 @@ struct RepDev {
   int32_t cellbase, ncells;  // cell arrays: [cellbase, cellbase + ncells] (last entry is the sentinel)
   int32_t nc[3];
   int32_t tile0, ntiles;
-  int32_t chunk0, nchunks;
+  int32_t chunk0, nchunks;   // record-reduction chunks over this replica's atom groups
+  int32_t cc0, ncc;          // cell-scan chunks (kCellChunk cells each)
   double L[3], cs[3];
   float csf[3];
   float pad0;
@@ -68,6 +70,7 @@ struct Eng {
   int32_t R, maxnb;
   int64_t S;  // slots
   int32_t T, C, nchunks_total;
+  int32_t tpa, G, NG;  // threads per atom, atoms per warp (32/tpa), atom groups (S/G)
   RepDev* rep;
   int32_t* active;
   int32_t* flag;
@@ -77,14 +80,23 @@ struct Eng {
   int32_t *nbr, *nnb;
   int32_t *tile_rep, *cell_rep;
   int32_t *chunk_rep, *chunk_tile0, *chunk_ntiles;
+  int32_t ncc;
+  int32_t *cc_rep, *cc_c0, *cc_n, *cc_sum;
   double *xa, *tmp_xa, *tmp_v;
-  int32_t *tmp_cell, *tmp_id, *tmp_sp, *newcell, *perm;
+  int32_t *tmp_cell, *tmp_id, *tmp_sp, *newcell, *perm, *perm2;
   int32_t *count, *start, *cursor;
   double *partials, *chunk_part, *rec;
   int32_t rec_cap;
   acs_dev_status* status;
   unsigned int* bar;  // [0] counter, [1] generation
+  unsigned long long* phase_ns;  // rebuild phase durations, accumulated (block 0 timestamps)
 };
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ double py_mod(double x, double L) {
   double r = fmod(x, L);
@@ -145,18 +157,85 @@ __device__ bool grid_sync(unsigned int* bar, acs_dev_status* st) {
 }
 
 // ------------------------------------------------------------------------------- pair kernel --
+// Per-pair coefficients: either the single-species constants (ONE) or the species-pair tables.
+struct PairK {
+  float eps4, eps24, sig2, rc2, ushift, qqk;
+};
+
+template <bool ONE>
+__device__ __forceinline__ PairK pair_consts(const FFDev& ff, int p, const PairK& c1) {
+  if (ONE) return c1;
+  PairK k;
+  k.eps4 = ff.lj_eps4[p];
+  k.eps24 = ff.lj_eps24[p];
+  k.sig2 = ff.lj_sig2[p];
+  k.rc2 = ff.lj_rc2[p];
+  k.ushift = ff.lj_ushift[p];
+  k.qqk = ff.qqk[p];
+  return k;
+}
+
+// One pair: accumulate f_i += coef * d (Kahan) and, when recording, the pair energy (Kahan).
+template <bool LJ, bool DSF, bool REC, bool ONE>
+__device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int sio, const float4& pi, uint32_t e,
+                                          const float4& pj, const float4* shift_row, float& fx, float& fy, float& fz,
+                                          float& cx, float& cy, float& cz, float& eu, float& ce) {
+  const float4 sh = shift_row[e >> kIdxBits];
+  const float dx = (pj.x - pi.x) + sh.x;
+  const float dy = (pj.y - pi.y) + sh.y;
+  const float dz = (pj.z - pi.z) + sh.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const PairK k = pair_consts<ONE>(ff, ONE ? 0 : sio + __float_as_int(pj.w), c1);
+  float coef = 0.f;
+  if (LJ) {
+    if (r2 < k.rc2) {
+      const float ir2 = __frcp_rn(r2);
+      const float sr2 = k.sig2 * ir2;
+      const float sr6 = sr2 * sr2 * sr2;
+      coef = -k.eps24 * ir2 * sr6 * (2.0f * sr6 - 1.0f);
+      if (REC) kahan_add(eu, ce, k.eps4 * (sr6 * sr6 - sr6) - k.ushift);
+    }
+  }
+  if (DSF) {
+    if (r2 < ff.dsf_rc2) {
+      const float ir = rsqrtf(r2);
+      const float rr = r2 * ir;
+      const float ar = ff.dsf_a * rr;
+      const float er = erfcf(ar);
+      coef -= k.qqk * ((er * ir * ir + ff.dsf_c * __expf(-ar * ar) * ir) - ff.dsf_fshift) * ir;
+      if (REC) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
+    }
+  }
+  kahan_add(fx, cx, coef * dx);
+  kahan_add(fy, cy, coef * dy);
+  kahan_add(fz, cz, coef * dz);
+}
+
 // MODE 0: step (force, kick, record?, kick, drift, image, skin test); 1: last step of a block (force,
 // kick, record?, store acceleration); 2: force only (acceleration + records, no kicks).
-template <bool LJ, bool DSF, bool REC, int MODE>
-__global__ void __launch_bounds__(256) k_step(Eng E, FFDev ff, int src, int dst) {
+// A warp handles G = 32/tpa atoms; the tpa lanes of an atom split its neighbour list (lane = phase*G +
+// atom-in-group, so each batch of list reads is one coalesced 128-byte row) and their Kahan partial sums
+// are combined in FP64 by a fixed xor-shuffle tree (deterministic).
+template <bool LJ, bool DSF, bool REC, int MODE, bool ONE>
+__global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int dst) {
   __shared__ float4 shift_tab[8][27];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
   if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
   const float4* __restrict__ imgs = E.img[src];
+  const int G = E.G, tpa = E.tpa;
+  const int sub_i = lane % G, phase = lane / G;
+  PairK c1;
+  c1.eps4 = ff.lj_eps4[0];
+  c1.eps24 = ff.lj_eps24[0];
+  c1.sig2 = ff.lj_sig2[0];
+  c1.rc2 = ff.lj_rc2[0];
+  c1.ushift = ff.lj_ushift[0];
+  c1.qqk = ff.qqk[0];
   int cur_rep = -1;
-  for (int tile = blockIdx.x * wpb + wib; tile < E.T; tile += gridDim.x * wpb) {
-    const int r = E.tile_rep[tile];
+  for (int w = blockIdx.x * wpb + wib; w < E.NG; w += gridDim.x * wpb) {
+    const int64_t i = (int64_t)w * G + sub_i;
+    const int r = E.tile_rep[i >> 5];
     if (!E.active[r]) continue;
     const RepDev& R = E.rep[r];
     if (r != cur_rep) {
@@ -168,55 +247,61 @@ __global__ void __launch_bounds__(256) k_step(Eng E, FFDev ff, int src, int dst)
       __syncwarp();
       cur_rep = r;
     }
-    const int64_t i = (int64_t)tile * 32 + lane;
     const bool valid = (i - R.atom0) < R.n;
     double rv[kRecW] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double dfx = 0.0, dfy = 0.0, dfz = 0.0, deu = 0.0;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int si = 0;
     if (valid) {
-      const float4 pi = imgs[i];
-      const int si = __float_as_int(pi.w);
+      pi = imgs[i];
+      si = __float_as_int(pi.w);
       const int sio = si * ACS_MAX_SPECIES;
+      const float4* shift_row = shift_tab[wib];
       float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, eu = 0.f, ce = 0.f;
       const int m = E.nnb[i];
-      const int32_t* __restrict__ lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
-#pragma unroll 2
-      for (int k = 0; k < m; ++k) {
-        const uint32_t e = (uint32_t)__ldg(lst + (int64_t)k * 32);
-        const float4 pj = __ldg(imgs + (e & kIdxMask));
-        const float4 sh = shift_tab[wib][e >> kIdxBits];
-        const float dx = (pj.x - pi.x) + sh.x;
-        const float dy = (pj.y - pi.y) + sh.y;
-        const float dz = (pj.z - pi.z) + sh.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const int p = sio + __float_as_int(pj.w);
-        float coef = 0.f;  // f_i += coef * d
-        if (LJ) {
-          if (r2 < ff.lj_rc2[p]) {
-            const float ir2 = 1.0f / r2;
-            const float sr2 = ff.lj_sig2[p] * ir2;
-            const float sr6 = sr2 * sr2 * sr2;
-            coef = -ff.lj_eps24[p] * ir2 * sr6 * (2.0f * sr6 - 1.0f);
-            if (REC) kahan_add(eu, ce, ff.lj_eps4[p] * (sr6 * sr6 - sr6) - ff.lj_ushift[p]);
-          }
-        }
-        if (DSF) {
-          if (r2 < ff.dsf_rc2) {
-            const float rr = sqrtf(r2);
-            const float ir = 1.0f / rr;
-            const float ar = ff.dsf_a * rr;
-            const float er = erfcf(ar);
-            const float qq = ff.qqk[p];
-            coef -= qq * ((er * ir * ir + ff.dsf_c * __expf(-ar * ar) * ir) - ff.dsf_fshift) * ir;
-            if (REC) kahan_add(eu, ce, qq * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
-          }
-        }
-        kahan_add(fx, cx, coef * dx);
-        kahan_add(fy, cy, coef * dy);
-        kahan_add(fz, cz, coef * dz);
+      const int n_it = m > phase ? (m - phase + tpa - 1) / tpa : 0;  // this lane's share of the list
+      const int32_t* __restrict__ lst = E.nbr + (int64_t)w * E.maxnb * G + lane;  // entry phase + t*tpa at t*32
+      const int n4 = n_it & ~3;
+      uint32_t en[4] = {0u, 0u, 0u, 0u};
+      if (n4 > 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) en[q] = (uint32_t)__ldcs(lst + q * 32);
       }
+      int t = 0;
+      for (; t < n4; t += 4) {
+        uint32_t e[4];
+        float4 pj[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = en[q];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & kIdxMask));
+        if (t + 4 < n4) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) en[q] = (uint32_t)__ldcs(lst + (t + 4 + q) * 32);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e[q], pj[q], shift_row, fx, fy, fz, cx, cy, cz, eu, ce);
+      }
+      for (; t < n_it; ++t) {
+        const uint32_t e = (uint32_t)__ldcs(lst + t * 32);
+        const float4 pj = __ldg(imgs + (e & kIdxMask));
+        pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e, pj, shift_row, fx, fy, fz, cx, cy, cz, eu, ce);
+      }
+      dfx = (double)fx - (double)cx;
+      dfy = (double)fy - (double)cy;
+      dfz = (double)fz - (double)cz;
+      deu = (double)eu - (double)ce;
+    }
+    for (int off = G; off < 32; off <<= 1) {
+      dfx += __shfl_xor_sync(0xffffffffu, dfx, off);
+      dfy += __shfl_xor_sync(0xffffffffu, dfy, off);
+      dfz += __shfl_xor_sync(0xffffffffu, dfz, off);
+      if (REC) deu += __shfl_xor_sync(0xffffffffu, deu, off);
+    }
+    if (valid && phase == 0) {
       const double im = ff.inv_mass[si];
-      const double ax = ((double)fx - (double)cx) * im;
-      const double ay = ((double)fy - (double)cy) * im;
-      const double az = ((double)fz - (double)cz) * im;
+      const double ax = dfx * im, ay = dfy * im, az = dfz * im;
       if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
       double vx = E.v[3 * i], vy = E.v[3 * i + 1], vz = E.v[3 * i + 2];
       if (MODE != 2) {
@@ -227,15 +312,15 @@ __global__ void __launch_bounds__(256) k_step(Eng E, FFDev ff, int src, int dst)
       if (REC) {
         const double ms = ff.mass[si];
         rv[0] = 0.5 * ms * (vx * vx + vy * vy + vz * vz);
-        rv[1] = 0.5 * ((double)eu - (double)ce) - (DSF ? ff.self_e[si] : 0.0);
+        rv[1] = 0.5 * deu - (DSF ? ff.self_e[si] : 0.0);
         const double px = ms * vx, py = ms * vy, pz = ms * vz;
         rv[2] = px;
         rv[3] = py;
         rv[4] = pz;
-        int c0, c1, c2;
-        cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
+        int c0, c1i, c2;
+        cell_coords(E.cellid[i] - R.cellbase, R, c0, c1i, c2);
         const double x = py_mod(c0 * R.cs[0] + E.u[3 * i], R.L[0]);
-        const double y = py_mod(c1 * R.cs[1] + E.u[3 * i + 1], R.L[1]);
+        const double y = py_mod(c1i * R.cs[1] + E.u[3 * i + 1], R.L[1]);
         const double z = py_mod(c2 * R.cs[2] + E.u[3 * i + 2], R.L[2]);
         rv[5] = y * pz - z * py;
         rv[6] = z * px - x * pz;
@@ -265,11 +350,11 @@ __global__ void __launch_bounds__(256) k_step(Eng E, FFDev ff, int src, int dst)
     }
     if (REC) {
 #pragma unroll
-      for (int w = 0; w < kRecW; ++w) {
-        double x = rv[w];
+      for (int q = 0; q < kRecW; ++q) {
+        double x = rv[q];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) E.partials[(int64_t)tile * kRecW + w] = x;
+        if (lane == 0) E.partials[(int64_t)w * kRecW + q] = x;
       }
     }
   }
@@ -340,7 +425,7 @@ __device__ int block_scan_excl(int v, int* total) {
 
 // Rebuild of flagged replicas and per-replica record reduction. Cooperative launch (all blocks resident);
 // every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging.
-__global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
+__global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
   __shared__ unsigned char fl[kMaxRep];
   __shared__ int any_s;
   if (threadIdx.x == 0) any_s = 0;
@@ -380,7 +465,15 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     }
   }
   if (!any || err0) return;
-  if (!grid_sync(E.bar, E.status)) return;  // every block has read the flags before they are cleared
+  unsigned long long t_prev = (blockIdx.x == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
+#define PHASE(k)                                                  \
+  if (blockIdx.x == 0 && threadIdx.x == 0) {                      \
+    const unsigned long long t_now = gtimer();                    \
+    atomicAdd(&E.phase_ns[k], t_now - t_prev);                    \
+    t_prev = t_now;                                               \
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  PHASE(1);
 
   // P0: clear counters of flagged replicas' cells
   for (int64_t c = gtid; c < E.C; c += gstride) {
@@ -390,6 +483,7 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     }
   }
   if (!grid_sync(E.bar, E.status)) return;
+  PHASE(2);
   // P1: absolute wrapped positions and new cells
   for (int64_t s = gtid; s < E.S; s += gstride) {
     const int r = E.tile_rep[s >> 5];
@@ -420,26 +514,53 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     atomicAdd(&E.count[c], 1);
   }
   if (!grid_sync(E.bar, E.status)) return;
-  // P2: per-replica exclusive scan of cell counts -> slot starts; clear flags; count rebuilds
-  for (int r = blockIdx.x; r < E.R; r += gridDim.x) {
-    if (!fl[r]) continue;
-    const RepDev& R = E.rep[r];
-    int carry = 0;
-    for (int b = 0; b < R.ncells; b += blockDim.x) {
-      const int c = b + threadIdx.x;
-      const int v = c < R.ncells ? E.count[R.cellbase + c] : 0;
-      int total;
-      const int ex = block_scan_excl(v, &total);
-      if (c < R.ncells) E.start[R.cellbase + c] = (int32_t)(R.atom0 + carry + ex);
-      carry += total;
+  PHASE(3);
+  // P2: exclusive scan of cell counts -> slot starts, in fixed 1024-cell chunks: (a) chunk-local scans,
+  // (b) per-replica prefix of chunk totals (also: sentinel, clear flag, count the rebuild), (c) offsets.
+  for (int c = blockIdx.x; c < E.ncc; c += gridDim.x) {
+    if (!fl[E.cc_rep[c]]) continue;
+    const int c0 = E.cc_c0[c], nc = E.cc_n[c];
+    int v[4], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = 4 * threadIdx.x + q;
+      v[q] = idx < nc ? E.count[c0 + idx] : 0;
+      sum += v[q];
     }
-    if (threadIdx.x == 0) {
-      E.start[R.cellbase + R.ncells] = (int32_t)(R.atom0 + R.n);
-      E.flag[r] = 0;
-      atomicAdd(&E.status->rebuilds, 1);
+    int total;
+    int ex = block_scan_excl(sum, &total);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = 4 * threadIdx.x + q;
+      if (idx < nc) E.start[c0 + idx] = ex;
+      ex += v[q];
     }
+    if (threadIdx.x == 0) E.cc_sum[c] = total;
   }
   if (!grid_sync(E.bar, E.status)) return;
+  PHASE(4);
+  for (int64_t r = gtid; r < E.R; r += gstride) {
+    if (!fl[r]) continue;
+    const RepDev& R = E.rep[r];
+    int64_t off = R.atom0;
+    for (int c = R.cc0; c < R.cc0 + R.ncc; ++c) {
+      const int t = E.cc_sum[c];
+      E.cc_sum[c] = (int32_t)off;
+      off += t;
+    }
+    E.start[R.cellbase + R.ncells] = (int32_t)(R.atom0 + R.n);
+    E.flag[r] = 0;
+    atomicAdd(&E.status->rebuilds, 1);
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  PHASE(5);
+  for (int c = blockIdx.x; c < E.ncc; c += gridDim.x) {
+    if (!fl[E.cc_rep[c]]) continue;
+    const int c0 = E.cc_c0[c], nc = E.cc_n[c], add_v = E.cc_sum[c];
+    for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) E.start[c0 + idx] += add_v;
+  }
+  if (!grid_sync(E.bar, E.status)) return;
+  PHASE(6);
   // P3: scatter old slots to new slots
   for (int64_t s = gtid; s < E.S; s += gstride) {
     const int r = E.tile_rep[s >> 5];
@@ -448,29 +569,25 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     E.perm[E.start[c] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
   }
   if (!grid_sync(E.bar, E.status)) return;
-  // P3b: deterministic order inside each cell (ascending old slot)
-  for (int64_t c = gtid; c < E.C; c += gstride) {
-    const int r = E.cell_rep[c];
-    if (!fl[r]) continue;
-    const RepDev& R = E.rep[r];
-    if (c == R.cellbase + R.ncells) continue;  // sentinel
+  PHASE(7);
+  // P3b: deterministic order inside each cell: every atom's rank among its cell's atoms by old slot
+  for (int64_t k = gtid; k < E.S; k += gstride) {
+    const int r = E.tile_rep[k >> 5];
+    if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
+    const int v = E.perm[k];
+    const int c = E.newcell[v];
     const int a0 = E.start[c], a1 = E.start[c + 1];
-    for (int a = a0 + 1; a < a1; ++a) {
-      const int v = E.perm[a];
-      int b = a - 1;
-      while (b >= a0 && E.perm[b] > v) {
-        E.perm[b + 1] = E.perm[b];
-        --b;
-      }
-      E.perm[b + 1] = v;
-    }
+    int rank = 0;
+    for (int a = a0; a < a1; ++a) rank += (E.perm[a] < v);
+    E.perm2[a0 + rank] = v;
   }
   if (!grid_sync(E.bar, E.status)) return;
+  PHASE(8);
   // P4: gather into new order
   for (int64_t k = gtid; k < E.S; k += gstride) {
     const int r = E.tile_rep[k >> 5];
     if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
-    const int o = E.perm[k];
+    const int o = E.perm2[k];
     E.tmp_cell[k] = E.newcell[o];
     E.tmp_id[k] = E.id[o];
     E.tmp_sp[k] = E.sp[o];
@@ -481,6 +598,7 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     }
   }
   if (!grid_sync(E.bar, E.status)) return;
+  PHASE(9);
   // P5: commit; offsets from the new cell origins; images
   for (int64_t k = gtid; k < E.S; k += gstride) {
     const int r = E.tile_rep[k >> 5];
@@ -507,56 +625,124 @@ __global__ void __launch_bounds__(256) k_rebuild(Eng E, int dst, int rec, int re
     E.img[dst][k] = make_img(ux, uy, uz, E.tmp_sp[k]);
   }
   if (!grid_sync(E.bar, E.status)) return;
-  // P6: neighbour lists with the reference's FP64 filter; image shift codes
-  for (int64_t i = gtid; i < E.S; i += gstride) {
-    const int r = E.tile_rep[i >> 5];
-    if (!fl[r]) continue;
-    const RepDev& R = E.rep[r];
-    if (i - R.atom0 >= R.n) continue;
-    int c0, c1, c2;
-    cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
-    const double xi = E.tmp_xa[3 * i], yi = E.tmp_xa[3 * i + 1], zi = E.tmp_xa[3 * i + 2];
-    const double uxi = E.u[3 * i], uyi = E.u[3 * i + 1], uzi = E.u[3 * i + 2];
-    int lo0, hi0, lo1, hi1, lo2, hi2;
-    stencil(c0, R.nc[0], lo0, hi0);
-    stencil(c1, R.nc[1], lo1, hi1);
-    stencil(c2, R.nc[2], lo2, hi2);
-    int cnt = 0;
-    bool bad = false;
-    int32_t* lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
-    for (int a = lo0; a <= hi0; ++a) {
-      const int n0 = wrapc(c0 + a, R.nc[0]);
-      for (int b = lo1; b <= hi1; ++b) {
-        const int n1 = wrapc(c1 + b, R.nc[1]);
-        for (int d = lo2; d <= hi2; ++d) {
-          const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + wrapc(c2 + d, R.nc[2]);
-          for (int k = E.start[cc], ke = E.start[cc + 1]; k < ke; ++k) {
-            if (k == i) continue;
-            double dx = sub(E.tmp_xa[3 * k], xi), dy = sub(E.tmp_xa[3 * k + 1], yi), dz = sub(E.tmp_xa[3 * k + 2], zi);
-            dx = min_image(dx, R.L[0]);
-            dy = min_image(dy, R.L[1]);
-            dz = min_image(dz, R.L[2]);
-            if (norm2(dx, dy, dz) < R.rl2) {
-              const int mx = (int)rint((dx - (E.u[3 * k] - uxi)) / R.cs[0]);
-              const int my = (int)rint((dy - (E.u[3 * k + 1] - uyi)) / R.cs[1]);
-              const int mz = (int)rint((dz - (E.u[3 * k + 2] - uzi)) / R.cs[2]);
-              const bool out = (mx < -1 || mx > 1 || my < -1 || my > 1 || mz < -1 || mz > 1);
-              bad |= out;  // reported as an error; the stored code stays inside the 27-entry shift table
-              const uint32_t code = out ? 13u : (uint32_t)((mx + 1) + 3 * (my + 1) + 9 * (mz + 1));
-              if (cnt < E.maxnb) lst[(int64_t)cnt * 32] = (int32_t)((uint32_t)k | (code << kIdxBits));
-              ++cnt;
+  PHASE(10);
+  // P6: neighbour lists in one pass over the 27-cell stencil. Each candidate's r^2 is first computed in
+  // FP32 from the new images (relative error ~1e-6): outside rl^2 (1 + 1e-4) it is rejected, inside
+  // rl^2 (1 - 1e-4) accepted; only the band between is decided by the reference's FP64 filter. So the
+  // pair set is exactly the FP64 filter's. That filter takes the minimum image by comparison with box/2,
+  // which for every pair that can lie inside the list radius (< box/2) is the IEEE result of
+  // d - box*round(d/box). The image shift stored with j is the stencil offset (>= 3 cells per edge) or
+  // minus the wrap (1 cell per edge).
+  {
+    const float4* __restrict__ im = E.img[dst];
+    const int G = E.G;
+    for (int64_t i = gtid; i < E.S; i += gstride) {
+      const int r = E.tile_rep[i >> 5];
+      if (!fl[r]) continue;
+      const RepDev& R = E.rep[r];
+      if (i - R.atom0 >= R.n) continue;
+      int c0, c1, c2;
+      cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
+      const float4 pi = im[i];
+      const float rl2f = (float)R.rl2;
+      const float lo_f = rl2f * (1.0f - 1e-4f), hi_f = rl2f * (1.0f + 1e-4f);
+      const float Lf0 = (float)R.L[0], Lf1 = (float)R.L[1], Lf2 = (float)R.L[2];
+      const bool one0 = R.nc[0] < 3, one1 = R.nc[1] < 3, one2 = R.nc[2] < 3;
+      const bool any_one = one0 || one1 || one2;
+      int lo0, hi0, lo1, hi1, lo2, hi2;
+      stencil(c0, R.nc[0], lo0, hi0);
+      stencil(c1, R.nc[1], lo1, hi1);
+      stencil(c2, R.nc[2], lo2, hi2);
+      int32_t* lst = E.nbr + (i / G) * (int64_t)E.maxnb * G + (i % G);
+      int cnt = 0;
+      // exact decision for a band candidate k; returns the code or -1
+      auto exact = [&](int k, int a, int b, int d) -> int {
+        double dx = sub(E.tmp_xa[3 * k], E.tmp_xa[3 * i]);
+        double dy = sub(E.tmp_xa[3 * k + 1], E.tmp_xa[3 * i + 1]);
+        double dz = sub(E.tmp_xa[3 * k + 2], E.tmp_xa[3 * i + 2]);
+        const int kx = dx > 0.5 * R.L[0] ? 1 : (dx < -0.5 * R.L[0] ? -1 : 0);
+        const int ky = dy > 0.5 * R.L[1] ? 1 : (dy < -0.5 * R.L[1] ? -1 : 0);
+        const int kz = dz > 0.5 * R.L[2] ? 1 : (dz < -0.5 * R.L[2] ? -1 : 0);
+        if (kx) dx = sub(dx, kx > 0 ? R.L[0] : -R.L[0]);
+        if (ky) dy = sub(dy, ky > 0 ? R.L[1] : -R.L[1]);
+        if (kz) dz = sub(dz, kz > 0 ? R.L[2] : -R.L[2]);
+        if (!(norm2(dx, dy, dz) < R.rl2)) return -1;
+        const int mx = one0 ? -kx : a, my = one1 ? -ky : b, mz = one2 ? -kz : d;
+        return (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+      };
+      auto keep = [&](int k, int code) {
+        if (cnt < E.maxnb) lst[(int64_t)cnt * G] = (int32_t)((uint32_t)k | ((uint32_t)code << kIdxBits));
+        ++cnt;
+      };
+      for (int a = lo0; a <= hi0; ++a) {
+        const int n0 = wrapc(c0 + a, R.nc[0]);
+        const float sa = a * R.csf[0];
+        for (int b = lo1; b <= hi1; ++b) {
+          const int n1 = wrapc(c1 + b, R.nc[1]);
+          const float sb = b * R.csf[1];
+          for (int d = lo2; d <= hi2; ++d) {
+            const float sd = d * R.csf[2];
+            const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + wrapc(c2 + d, R.nc[2]);
+            const int k0 = E.start[cc], k1 = E.start[cc + 1];
+            const int scode = (a + 1) + 3 * (b + 1) + 9 * (d + 1);
+            if (!any_one) {
+              int k = k0;
+              for (; k + 2 <= k1; k += 2) {
+                const float4 pj0 = im[k], pj1 = im[k + 1];
+                const float x0 = (pj0.x - pi.x) + sa, y0 = (pj0.y - pi.y) + sb, z0 = (pj0.z - pi.z) + sd;
+                const float x1 = (pj1.x - pi.x) + sa, y1 = (pj1.y - pi.y) + sb, z1 = (pj1.z - pi.z) + sd;
+                const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
+                if (k != i && q0 < hi_f) {
+                  const int c = q0 <= lo_f ? scode : exact(k, a, b, d);
+                  if (c >= 0) keep(k, c);
+                }
+                if (k + 1 != i && q1 < hi_f) {
+                  const int c = q1 <= lo_f ? scode : exact(k + 1, a, b, d);
+                  if (c >= 0) keep(k + 1, c);
+                }
+              }
+              if (k < k1 && k != i) {
+                const float4 pj = im[k];
+                const float x = (pj.x - pi.x) + sa, y = (pj.y - pi.y) + sb, z = (pj.z - pi.z) + sd;
+                const float q = x * x + y * y + z * z;
+                if (q < hi_f) {
+                  const int c = q <= lo_f ? scode : exact(k, a, b, d);
+                  if (c >= 0) keep(k, c);
+                }
+              }
+            } else {
+              for (int k = k0; k < k1; ++k) {
+                if (k == i) continue;
+                const float4 pj = im[k];
+                float fx = (pj.x - pi.x) + sa, fy = (pj.y - pi.y) + sb, fz = (pj.z - pi.z) + sd;
+                int wx = 0, wy = 0, wz = 0;
+                if (one0) wx = fx > 0.5f * Lf0 ? 1 : (fx < -0.5f * Lf0 ? -1 : 0);
+                if (one1) wy = fy > 0.5f * Lf1 ? 1 : (fy < -0.5f * Lf1 ? -1 : 0);
+                if (one2) wz = fz > 0.5f * Lf2 ? 1 : (fz < -0.5f * Lf2 ? -1 : 0);
+                fx -= wx * Lf0;
+                fy -= wy * Lf1;
+                fz -= wz * Lf2;
+                const float q = fx * fx + fy * fy + fz * fz;
+                if (q < hi_f) {
+                  const int mx = one0 ? -wx : a, my = one1 ? -wy : b, mz = one2 ? -wz : d;
+                  const int c = q <= lo_f ? (mx + 1) + 3 * (my + 1) + 9 * (mz + 1) : exact(k, a, b, d);
+                  if (c >= 0) keep(k, c);
+                }
+              }
             }
           }
         }
       }
+      E.nnb[i] = min(cnt, E.maxnb);
+      if (cnt > E.maxnb) {
+        atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
+        atomicMax(&E.status->need_nbr, cnt);
+      }
     }
-    E.nnb[i] = min(cnt, E.maxnb);
-    if (cnt > E.maxnb) {
-      atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
-      atomicMax(&E.status->need_nbr, cnt);
-    }
-    if (bad) atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
   }
+  __syncthreads();
+  PHASE(15);
+#undef PHASE
 }
 
 // Scatter caller arrays (replica-concatenated, engine units) into slots; cell 0 origin so u = x.
@@ -639,9 +825,9 @@ __global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out)
     if (i - R.atom0 >= R.n) continue;
     const float4 pi = E.img[src][i];
     const int sio = __float_as_int(pi.w) * ACS_MAX_SPECIES;
-    const int32_t* lst = E.nbr + (i >> 5) * (int64_t)E.maxnb * 32 + (i & 31);
+    const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
     for (int k = 0; k < E.nnb[i]; ++k) {
-      const uint32_t e = (uint32_t)lst[(int64_t)k * 32];
+      const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
       const float4 pj = E.img[src][e & kIdxMask];
       const uint32_t code = e >> kIdxBits;
       const int mx = (int)(code % 3) - 1, my = (int)((code / 3) % 3) - 1, mz = (int)(code / 9) - 1;
@@ -690,8 +876,19 @@ struct Layout {
   }
 };
 
+int tpa_of(const acs_engine_config* cfg) {
+  const int t = cfg->tpa;
+  return (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32) ? t : (t == 0 ? 1 : -1);
+}
+
 void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<int64_t>& src0, int64_t& S, int32_t& T,
-          int32_t& C, int32_t& NCH, int& err) {
+          int32_t& C, int32_t& NCH, int32_t& NCC, int& err) {
+  const int tpa = tpa_of(cfg);
+  if (tpa < 0) {
+    err = ACS_ERR_ARG;
+    return;
+  }
+  const int G = 32 / tpa;
   err = ACS_OK;
   reps.clear();
   src0.clear();
@@ -699,6 +896,7 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
   T = 0;
   C = 0;
   NCH = 0;
+  NCC = 0;
   int64_t g = 0;
   for (int r = 0; r < cfg->n_replicas; ++r) {
     const acs_replica& q = cfg->replicas[r];
@@ -734,7 +932,10 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     R.tile0 = (int32_t)(S / 32);
     R.ntiles = R.npad / 32;
     R.chunk0 = NCH;
-    R.nchunks = (R.ntiles + kChunkTiles - 1) / kChunkTiles;
+    R.nchunks = (R.npad / G + kChunkTiles - 1) / kChunkTiles;
+    R.cc0 = NCC;
+    R.ncc = (int32_t)((ncell + kCellChunk - 1) / kCellChunk);
+    NCC += R.ncc;
     R.dt = q.dt;
     R.hdt = 0.5 * q.dt;
     R.hs2 = q.half_skin * q.half_skin;
@@ -753,7 +954,8 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
   }
 }
 
-Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int32_t maxnb, int32_t rec_cap) {
+Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int32_t NCC, int32_t maxnb,
+                   int32_t rec_cap, int64_t NG) {
   Layout L;
   L.add(sizeof(RepDev) * R);                 // 0 rep
   L.add(4 * (size_t)R);                      // 1 active
@@ -785,12 +987,18 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(4 * (size_t)C);                      // 27 count
   L.add(4 * (size_t)C);                      // 28 start
   L.add(4 * (size_t)C);                      // 29 cursor
-  L.add(8 * (size_t)T * kRecW);              // 30 partials
+  L.add(8 * (size_t)NG * kRecW);             // 30 partials (one row per atom group)
   L.add(8 * (size_t)NCH * kRecW);            // 31 chunk partials
   L.add(8 * (size_t)rec_cap * R * kRecW);    // 32 records
   L.add(sizeof(acs_dev_status));             // 33 status
   L.add(16);                                 // 34 barrier
   L.add(8 * (size_t)R);                      // 35 src0
+  L.add(4 * (size_t)NCC);                    // 36 cc_rep
+  L.add(4 * (size_t)NCC);                    // 37 cc_c0
+  L.add(4 * (size_t)NCC);                    // 38 cc_n
+  L.add(4 * (size_t)NCC);                    // 39 cc_sum
+  L.add(8 * 16);                             // 40 phase timers
+  L.add(4 * (size_t)S);                      // 41 perm2
   return L;
 }
 
@@ -839,25 +1047,31 @@ FFDev make_ff(const acs_forcefield& f, int& err) {
   return ff;
 }
 
-template <bool LJ, bool DSF>
+template <bool LJ, bool DSF, bool ONE>
 int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
   dim3 g(e->step_blocks), b(e->step_threads);
   if (mode == 0) {
-    if (rec) k_step<LJ, DSF, true, 0><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
-    else k_step<LJ, DSF, false, 0><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
   } else if (mode == 1) {
-    if (rec) k_step<LJ, DSF, true, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
-    else k_step<LJ, DSF, false, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    if (rec) k_step<LJ, DSF, true, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    else k_step<LJ, DSF, false, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
   } else {
-    k_step<LJ, DSF, true, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    k_step<LJ, DSF, true, 2, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
   }
   return launch_status();
 }
 
 int launch_step(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
-  if (e->ff.lj && e->ff.dsf) return launch_step_t<true, true>(e, rec, mode, src, dst, s);
-  if (e->ff.lj) return launch_step_t<true, false>(e, rec, mode, src, dst, s);
-  return launch_step_t<false, true>(e, rec, mode, src, dst, s);
+  const bool one = e->ff.ns == 1;
+  if (e->ff.lj && e->ff.dsf)
+    return one ? launch_step_t<true, true, true>(e, rec, mode, src, dst, s)
+               : launch_step_t<true, true, false>(e, rec, mode, src, dst, s);
+  if (e->ff.lj)
+    return one ? launch_step_t<true, false, true>(e, rec, mode, src, dst, s)
+               : launch_step_t<true, false, false>(e, rec, mode, src, dst, s);
+  return one ? launch_step_t<false, true, true>(e, rec, mode, src, dst, s)
+             : launch_step_t<false, true, false>(e, rec, mode, src, dst, s);
 }
 
 int launch_rebuild(acs_engine* e, int dst, int rec, int rec_idx, int force_all, cudaStream_t s) {
@@ -905,11 +1119,12 @@ size_t acs_engine_bytes(const acs_engine_config* cfg) {
   std::vector<RepDev> reps;
   std::vector<int64_t> src0;
   int64_t S;
-  int32_t T, C, NCH;
+  int32_t T, C, NCH, NCC;
   int err;
-  plan(cfg, reps, src0, S, T, C, NCH, err);
+  plan(cfg, reps, src0, S, T, C, NCH, NCC, err);
   if (err) return 0;
-  return make_layout(cfg->n_replicas, S, T, C, NCH, cfg->maxnb, std::max(cfg->rec_cap, 1)).total;
+  return make_layout(cfg->n_replicas, S, T, C, NCH, NCC, cfg->maxnb, std::max(cfg->rec_cap, 1),
+                     S / (32 / tpa_of(cfg))).total;
 }
 
 int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs_engine** out) {
@@ -919,9 +1134,9 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   if ((uintptr_t)mem & 255) return ACS_ERR_ARG;
   acs_engine* e = new acs_engine();
   int64_t S;
-  int32_t T, C, NCH;
+  int32_t T, C, NCH, NCC;
   int err;
-  plan(cfg, e->reps, e->src0, S, T, C, NCH, err);
+  plan(cfg, e->reps, e->src0, S, T, C, NCH, NCC, err);
   if (err) {
     delete e;
     return err;
@@ -932,7 +1147,9 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
     return err;
   }
   const int rec_cap = std::max(cfg->rec_cap, 1);
-  Layout L = make_layout(cfg->n_replicas, S, T, C, NCH, cfg->maxnb, rec_cap);
+  const int tpa = tpa_of(cfg);
+  const int G = 32 / tpa;
+  Layout L = make_layout(cfg->n_replicas, S, T, C, NCH, NCC, cfg->maxnb, rec_cap, S / G);
   if (bytes < L.total) {
     delete e;
     return ACS_ERR_WORKSPACE;
@@ -945,6 +1162,9 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.T = T;
   E.C = C;
   E.nchunks_total = NCH;
+  E.tpa = tpa;
+  E.G = G;
+  E.NG = (int32_t)(S / G);
   E.rec_cap = rec_cap;
   E.rep = (RepDev*)(b + L.off[0]);
   E.active = (int32_t*)(b + L.off[1]);
@@ -982,17 +1202,31 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.status = (acs_dev_status*)(b + L.off[33]);
   E.bar = (unsigned int*)(b + L.off[34]);
   e->src0_dev = (int64_t*)(b + L.off[35]);
+  E.ncc = NCC;
+  E.cc_rep = (int32_t*)(b + L.off[36]);
+  E.cc_c0 = (int32_t*)(b + L.off[37]);
+  E.cc_n = (int32_t*)(b + L.off[38]);
+  E.cc_sum = (int32_t*)(b + L.off[39]);
+  E.phase_ns = (unsigned long long*)(b + L.off[40]);
+  E.perm2 = (int32_t*)(b + L.off[41]);
 
   // host-built index tables
   std::vector<int32_t> tile_rep(T), cell_rep(C), chunk_rep(NCH), chunk_t0(NCH), chunk_nt(NCH);
+  std::vector<int32_t> cc_rep(NCC), cc_c0(NCC), cc_n(NCC);
   for (int r = 0; r < E.R; ++r) {
     const RepDev& R = e->reps[r];
     for (int t = 0; t < R.ntiles; ++t) tile_rep[R.tile0 + t] = r;
     for (int c = 0; c <= R.ncells; ++c) cell_rep[R.cellbase + c] = r;
+    for (int c = 0; c < R.ncc; ++c) {
+      cc_rep[R.cc0 + c] = r;
+      cc_c0[R.cc0 + c] = R.cellbase + c * kCellChunk;
+      cc_n[R.cc0 + c] = std::min(kCellChunk, R.ncells - c * kCellChunk);
+    }
     for (int c = 0; c < R.nchunks; ++c) {
       chunk_rep[R.chunk0 + c] = r;
-      chunk_t0[R.chunk0 + c] = R.tile0 + c * kChunkTiles;
-      chunk_nt[R.chunk0 + c] = std::min(kChunkTiles, R.ntiles - c * kChunkTiles);
+      const int g0 = (int)(R.atom0 / G), ng = R.npad / G;
+      chunk_t0[R.chunk0 + c] = g0 + c * kChunkTiles;
+      chunk_nt[R.chunk0 + c] = std::min(kChunkTiles, ng - c * kChunkTiles);
     }
   }
   std::vector<int32_t> ones(E.R, 1), zeros(E.R, 0);
@@ -1011,7 +1245,11 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   ok = ok && cudaMemcpy(E.status, &st0, sizeof(st0), cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.bar, bar0, 16, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(e->src0_dev, e->src0.data(), 8 * (size_t)E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.cc_rep, cc_rep.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.cc_c0, cc_c0.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.cc_n, cc_n.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemset(E.nnb, 0, 4 * (size_t)S) == cudaSuccess;
+  ok = ok && cudaMemset(E.phase_ns, 0, 8 * 16) == cudaSuccess;
   int sms = 0, per_sm = 0;
   ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev) == cudaSuccess;
   ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, 256, 0) == cudaSuccess;
@@ -1019,9 +1257,9 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
     delete e;
     return ACS_ERR_CUDA;
   }
-  e->coop_blocks = sms * std::min(per_sm, 2);
+  e->coop_blocks = sms * std::min(per_sm, 4);
   const int grid_mult = cfg->grid_mult > 0 ? cfg->grid_mult : 0;
-  const int64_t need = (S + 255) / 256;
+  const int64_t need = (S / G * 32 + 255) / 256;
   e->step_blocks = (int)(grid_mult ? std::min<int64_t>(need, (int64_t)sms * grid_mult) : need);
   if (e->step_blocks < 1) e->step_blocks = 1;
   *out = e;
@@ -1207,6 +1445,13 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
   out_ms[2] = (float)cnt[0];
   out_ms[3] = (float)cnt[1];
   return st;
+}
+
+int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear) {
+  if (!e || !out16) return ACS_ERR_ARG;
+  if (cudaMemcpy(out16, e->E.phase_ns, 8 * 16, cudaMemcpyDeviceToHost) != cudaSuccess) return ACS_ERR_CUDA;
+  if (clear && cudaMemset(e->E.phase_ns, 0, 8 * 16) != cudaSuccess) return ACS_ERR_CUDA;
+  return ACS_OK;
 }
 
 int acs_engine_destroy(acs_engine* e) {

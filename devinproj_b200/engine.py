@@ -47,7 +47,7 @@ class ForceField(C.Structure):
 
 class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
-                ("replicas", C.POINTER(Replica)), ("ff", ForceField)]
+                ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField)]
 
 
 class DevStatusC(C.Structure):
@@ -69,6 +69,7 @@ ENGINE_SIGNATURES = {
     "acs_engine_load_state": (C.c_int, [P, P, P, P]),
     "acs_engine_count_pairs": (C.c_int, [P, P, P]),
     "acs_engine_run_timed": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(C.c_float), P]),
+    "acs_engine_phase_times": (C.c_int, [P, P, C.c_int]),
     "acs_engine_destroy": (C.c_int, [P]),
 }
 _lib.SIGNATURES.update(ENGINE_SIGNATURES)
@@ -128,7 +129,7 @@ class _SpeciesView:
 class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
-    def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0):
+    def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -144,7 +145,8 @@ class Engine:
             self._reps[k].dt = float(r["dt"])
             self._reps[k].rlist = float(r["rlist"])
             self._reps[k].half_skin = float(r["half_skin"])
-        self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self._reps, ff)
+        self.tpa = int(tpa)
+        self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff)
         nbytes = L.acs_engine_bytes(C.byref(self.cfg))
         if nbytes == 0:
             raise ValueError("engine configuration rejected (sizes, list radius >= box/2, or too many replicas)")
@@ -211,6 +213,15 @@ class Engine:
                    "acs_engine_run_timed")
         return out[0] / max(out[2], 1), out[1] / max(out[3], 1), out[0] + out[1]
 
+    PHASES = {1: "flags", 2: "clear", 3: "bin", 4: "scan_a", 5: "scan_b", 6: "scan_c", 7: "scatter", 8: "sort",
+              9: "gather", 10: "commit", 15: "list_build_block0"}
+
+    def phase_times(self, clear=True):
+        """List-maintenance phase times (ms, accumulated) from the device global timer."""
+        out = np.zeros(16, dtype=np.uint64)
+        _lib.check(self.L.acs_engine_phase_times(self.h, out.ctypes.data, 1 if clear else 0), "phase_times")
+        return {name: float(out[k]) / 1e6 for k, name in self.PHASES.items()}
+
     def records(self, count: int) -> np.ndarray:
         """(count, R, 8) FP64 records [KE, PE, Px, Py, Pz, Lx, Ly, Lz] in engine units."""
         if count == 0:
@@ -252,15 +263,27 @@ def estimate_maxnb(n, box, rlist):
     return int(min(expected * 1.3 + 32, 4096) + 7) // 8 * 8
 
 
-def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0):
+def default_tpa(n_atoms_total, neighbors_per_atom):
+    """Threads per atom for the pair kernel: enough threads to fill the GPU (about 300k), no more lanes than
+    a quarter of the neighbour count per atom."""
+    tpa = 1
+    while tpa < 32 and n_atoms_total * tpa < 300_000 and tpa * 8 <= max(neighbors_per_atom, 1):
+        tpa *= 2
+    return tpa
+
+
+def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
     reps = [dict(n=r["n"], box=np.asarray(r["box"], float) / LEN, dt=r["dt"] / TIME, rlist=rlist / LEN,
                  half_skin=half_skin / LEN) for r in replicas_si]
+    expect = max(estimate_maxnb(r["n"], r["box"], r["rlist"]) for r in reps)
     if maxnb is None:
-        maxnb = max(estimate_maxnb(r["n"], r["box"], r["rlist"]) for r in reps)
-    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult), rlist, half_skin
+        maxnb = expect
+    if tpa is None:
+        tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3)
+    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa), rlist, half_skin
 
 
 def _upload_state(engine, systems):
@@ -276,7 +299,7 @@ def _upload_state(engine, systems):
     engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
 
 
-def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0):
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None):
     """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
     grows the neighbour capacity once if the first build overflows."""
     for s in systems:
@@ -285,7 +308,8 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0):
     species = systems[0].species
     reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
     for attempt in range(3):
-        eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult)
+        eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,
+                                      tpa=tpa)
         _upload_state(eng, systems)
         st = eng.status()
         if st.flags & _lib.FLAG_OVERFLOW:
@@ -308,7 +332,7 @@ class GpuSimulation:
     `run` call (and at records when positions=True)."""
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
-                 rec_cap=256, grid_mult=0):
+                 rec_cap=256, grid_mult=0, tpa=None):
         from .integrators import VelocityVerlet
         from .simulation import Trajectory
         from .units import si
@@ -329,7 +353,7 @@ class GpuSimulation:
         self._initial = None
         self.engine, self.rlist, self.half_skin = start_engine(
             [system], self.forces, [self.dt if self.dt is not None else 1e-15], maxnb=maxnb, rec_cap=rec_cap,
-            grid_mult=grid_mult)
+            grid_mult=grid_mult, tpa=tpa)
         self._last = self.engine.records(1)[0, 0]
         self._pull()
 
@@ -427,7 +451,7 @@ class GpuSimulation:
     def clone(self, dt=None):
         sim = GpuSimulation(self.system.copy(), self.forces, integrator=self.integrator,
                             dt=self.dt if dt is None else dt, seed=self.seed, maxnb=self.engine.maxnb,
-                            rec_cap=self.engine.rec_cap)
+                            rec_cap=self.engine.rec_cap, tpa=self.engine.tpa)
         return sim
 
     def accuracy_report(self, convergence_duration=None):
@@ -446,4 +470,4 @@ class _InitialState:
     def clone(self, dt=None):
         s = self._sim
         return GpuSimulation(self.system.copy(), s.forces, integrator=s.integrator, dt=s.dt if dt is None else dt,
-                             seed=s.seed, maxnb=s.engine.maxnb, rec_cap=s.engine.rec_cap)
+                             seed=s.seed, maxnb=s.engine.maxnb, rec_cap=s.engine.rec_cap, tpa=s.engine.tpa)

@@ -46,6 +46,8 @@ typedef struct acs_engine_config {
   int32_t maxnb;      /* neighbour capacity per atom */
   int32_t rec_cap;    /* records kept per run call */
   int32_t grid_mult;  /* step kernel: blocks per SM (0 = one thread per atom slot) */
+  int32_t tpa;        /* threads per atom in the pair kernel: 1, 2, 4, 8, 16 or 32 (0 = 1) */
+  int32_t pad;
   const acs_replica* replicas;  /* host array */
   acs_forcefield ff;
 } acs_engine_config;
@@ -79,6 +81,10 @@ int acs_engine_launch_info(acs_engine* e, int32_t* step_blocks, int32_t* coop_bl
 /* The launch sequence of one block, eager, with CUDA events around every kernel (synchronous):
  * out_ms = {step-kernel ms total, list-maintenance ms total, step launches, list-maintenance launches}. */
 int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, float* out_ms, void* stream);
+/* Accumulated wall time (ns, device global timer, block 0's view) of the list-maintenance phases:
+ * [1] flag read, [2] clear, [3] bin, [4..6] scan, [7] scatter, [8] in-cell sort, [9] gather, [10] commit,
+ * [15] list build (block 0 share). Synchronous. */
+int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear);
 int acs_engine_destroy(acs_engine* e);
 
 #ifdef __cplusplus
