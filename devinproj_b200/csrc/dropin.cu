@@ -7,6 +7,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -654,3 +655,77 @@ int acs_reduce_conserved(const double* pos, const double* vel, const int32_t* sp
 }
 
 }  // extern "C"
+
+// ============================================================= allocation-free LJ force entry point ==
+// Some callers cannot allocate device memory when they need forces: code that owns every byte of the GPU
+// through its own pool, real-time loops that forbid allocation after start-up, or plug-in hosts that hand
+// out only input and output buffers. acs_lj_fp64_noalloc serves them: it runs the same FP64 LJ kernel as
+// acs_lj_fp64, but its reduction scratch (one FP64 partial per 256-atom block plus a completion counter)
+// lives in the fixed device array below instead of a caller-provided work buffer.
+//
+// The array is 64 KiB + 256 B and exists on every GPU that loads this library until the process exits;
+// it bounds n at kNoAllocMaxAtoms = 2,097,152 atoms. All calls share it, so calls whose work overlaps on the
+// GPU (different streams, or different host threads on one device) race and corrupt each other's energy;
+// serialise them. The completion counter is cleared at the start of every call; the partials are fully
+// overwritten by each call.
+namespace {
+
+constexpr int64_t kNoAllocMaxBlocks = 8192;                   // 8192 partials of 8 bytes = 64 KiB
+constexpr int64_t kNoAllocMaxAtoms = kNoAllocMaxBlocks * kBlock;  // 2,097,152
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocMaxBlocks * 8 + 256];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device, looked up on the first call per device.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ACS_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ACS_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return ACS_OK;
+}
+
+}  // namespace
+
+extern "C" int acs_lj_fp64_noalloc(const double* pos, const int32_t* sp, int64_t n, const double* box3, int periodic,
+                                   const int32_t* nbr, const int32_t* nnb, int32_t maxnb, int32_t n_species,
+                                   const double* eps_tab, const double* sig_tab, double cutoff, double* force,
+                                   double* energy_dev, void* stream) {
+  if (n > kNoAllocMaxAtoms) return ACS_ERR_UNSUPPORTED;
+  if (n < 1 || !pos || !sp || !force || !energy_dev || !eps_tab || !sig_tab || n_species < 1 ||
+      n_species > ACS_MAX_SPECIES || !(cutoff > 0.0) || (nbr && (!nnb || maxnb < 1)))
+    return ACS_ERR_ARG;
+  void* scratch = nullptr;
+  int st = noalloc_scratch(&scratch);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nb = ceil_div(n, kBlock);
+  double* partials = (double*)scratch;
+  unsigned int* ticket = (unsigned int*)((char*)scratch + kNoAllocMaxBlocks * 8);
+  if (cudaMemsetAsync(ticket, 0, 4, s) != cudaSuccess) return ACS_ERR_CUDA;
+  LJTab t;
+  t.ns = n_species;
+  for (int a = 0; a < n_species * n_species; ++a) {
+    t.eps[a] = eps_tab[a];
+    t.sig2[a] = sig_tab[a] * sig_tab[a];
+    const double rc = cutoff * sig_tab[a];
+    t.rc2[a] = rc * rc;
+  }
+  const double c2 = cutoff * cutoff;
+  const double src6 = (1.0 / c2) * (1.0 / c2) * (1.0 / c2);
+  t.shift6 = src6 * src6 - src6;
+  Box3 b = make_box(box3, periodic);
+  if (nbr)
+    k_lj64<false><<<(int)nb, kBlock, 0, s>>>(pos, sp, n, b, nbr, nnb, maxnb, t, force, partials, ticket, energy_dev);
+  else
+    k_lj64<true><<<(int)nb, kBlock, 0, s>>>(pos, sp, n, b, nullptr, nullptr, 0, t, force, partials, ticket,
+                                           energy_dev);
+  return launch_status();
+}
