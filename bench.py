@@ -35,6 +35,15 @@ FALLBACK_HBM_GBS = 6650.0
 def workload(name, seed=0):
     from devinproj_b200 import configs
     cfg = workload_meta(name)
+    if name == "ensemble":
+        nc = configs.replica_sizes(256, seed=seed)
+        systems, dts = [], []
+        for k, c in enumerate(nc):
+            sys_k, lj = configs.lj_fluid(int(c), seed=1000 * seed + k)
+            for f in (1, 2, 4):
+                systems.append(sys_k.copy())
+                dts.append(0.005 * configs.AR_TAU / f)
+        return systems, [lj], dts, cfg
     if name == "lj1m":
         s, forces, dt = configs.lj_large(64, seed=seed)
     elif name == "nacl4096":
@@ -187,11 +196,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--record-every", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tpa", type=int, default=None, help="threads per atom in the pair kernel (default: auto)")
+    ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
+                    "autotuner), default: size heuristic")
     ap.add_argument("--profile", action="store_true",
                     help="engine only: warm-up graph steps then --steps eager launches (for ncu), no timing legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.tpa not in (None, "auto"):
+        args.tpa = int(args.tpa)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -215,8 +227,10 @@ def main():
     from devinproj_b200.engine import ACC, LEN, VEL, start_engine
 
     s, forces, dt, cfg = workload(args.workload, seed=rank)
-    eng, rlist, hs = start_engine([s], forces, [dt], rec_cap=max(args.steps // args.record_every + 2, 4), tpa=args.tpa)
-    n = s.n
+    systems, dts = (s, dt) if isinstance(s, list) else ([s], [dt])
+    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=max(args.steps // args.record_every + 2, 4),
+                                  tpa=args.tpa)
+    n = sum(x.n for x in systems)
     pairs_lj, pairs_dsf = eng.count_pairs()
     step_blocks, coop_blocks, slots = eng.launch_info()
     init = eng.records(1)[0, 0].copy()
@@ -264,7 +278,7 @@ def main():
     ms = e0.elapsed_time(e1)
     st = eng.check("timed run")
     nrec = args.steps // args.record_every + (1 if args.steps % args.record_every else 0)
-    recs = eng.records(nrec)[:, 0, :]
+    recs_all = eng.records(nrec)                     # (records, replicas, 8), engine units
     rebuilds_timed = st.rebuilds - rb0
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -272,16 +286,23 @@ def main():
         ms = float(t.item())
     value = n * args.steps * world / (ms / 1e3)
 
-    # energy / momentum over the timed run (the report's metrics), in engine units
-    E = recs[:, 0] + recs[:, 1]
-    scale = max(abs(E[0]), np.max(np.abs(recs[:, 0])), np.max(np.abs(recs[:, 1])))
-    drift = float(np.max(np.abs(E - E[0])) / scale)
-    slope = float(np.polyfit(np.arange(len(E)) * args.record_every, E, 1)[0]) if len(E) > 2 else 0.0
+    # energy / momentum over the timed run (the report's metrics), worst replica
     pos_d, vel_d, acc_d = eng.get_state()
-    masses = np.array([x.mass for x in s.species])[s.sp]
-    pscale = float(np.sum(masses[:, None] * np.abs(vel_d.cpu().numpy() * VEL)))
-    P = recs[:, 2:5] * (1.66053906660e-27 * VEL)
-    mom_drift = float(np.max(np.linalg.norm(P - P[0], axis=1)) / pscale)
+    vel_np = vel_d.cpu().numpy() * VEL
+    drift = slope_rel = mom_drift = 0.0
+    for r in range(len(systems)):
+        recs = recs_all[:, r, :]
+        E = recs[:, 0] + recs[:, 1]
+        scale = max(abs(E[0]), np.max(np.abs(recs[:, 0])), np.max(np.abs(recs[:, 1])))
+        drift = max(drift, float(np.max(np.abs(E - E[0])) / scale))
+        if len(E) > 2:
+            slope_rel = max(slope_rel, abs(float(np.polyfit(np.arange(len(E)) * args.record_every, E, 1)[0])) / scale)
+        sr = systems[r]
+        o0, o1 = eng.offsets[r], eng.offsets[r + 1]
+        m_r = np.array([x.mass for x in sr.species])[sr.sp]
+        pscale = float(np.sum(m_r[:, None] * np.abs(vel_np[o0:o1])))
+        P = recs[:, 2:5] * (1.66053906660e-27 * VEL)
+        mom_drift = max(mom_drift, float(np.max(np.linalg.norm(P - P[0], axis=1)) / pscale))
 
     # ---------------------------------------------------------------- per-kernel timing (eager, events)
     k_step_ms, k_reb_ms, _ = eng.run_timed(min(args.steps, 1000), args.record_every)
@@ -289,16 +310,19 @@ def main():
     eng.check("timed eager run")
 
     # ---------------------------------------------------------------- accuracy vs the FP64 path
-    # FP64 forces on the final state by the drop-in kernels (pinned to the reference to 1e-12)
-    s.pos = pos_d.cpu().numpy() * LEN
-    s.vel = vel_d.cpu().numpy() * VEL
-    F32 = acc_d.cpu().numpy() * ACC * masses[:, None]
+    # FP64 forces on the final state by the drop-in kernels (pinned to the reference to 1e-12); the largest
+    # replica when there are several
+    r_chk = int(np.argmax([x.n for x in systems]))
+    sr = systems[r_chk]
+    o0, o1 = eng.offsets[r_chk], eng.offsets[r_chk + 1]
+    sr.pos = pos_d.cpu().numpy()[o0:o1] * LEN
+    sr.vel = vel_np[o0:o1]
+    m_r = np.array([x.mass for x in sr.species])[sr.sp]
+    F32 = acc_d.cpu().numpy()[o0:o1] * ACC * m_r[:, None]
     F64 = np.zeros_like(F32)
-    U64 = 0.0
     for f in forces:
-        Fi, Ui = f.compute(s)
+        Fi, _ = f.compute(sr)
         F64 += Fi
-        U64 += Ui
     f_err = float(np.sqrt(np.mean(np.sum((F32 - F64) ** 2, 1)) / np.mean(np.sum(F64 ** 2, 1))))
 
     # ---------------------------------------------------------------- end to end (host buffers)
@@ -356,7 +380,8 @@ def main():
         "vs_baseline": None, "dtype": "fp32-pairs/f64-state", "data": "synthetic (seeded fcc lattice, MB velocities)",
         "config": full_config(cfg, args, world),
         "accuracy": {"force_rms_rel_err_vs_fp64": f_err, "energy_drift_report_metric": drift,
-                     "energy_drift_per_step_rel": slope / scale if scale else 0.0,
+                     "drift_note": "max over replicas" if len(systems) > 1 else "single system",
+                     "energy_drift_per_step_rel": slope_rel,
                      "momentum_drift_report_metric": mom_drift, "steps_in_drift_window": args.steps,
                      "rebuilds_in_timed_region": int(rebuilds_timed)},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -388,6 +413,10 @@ WORKLOADS = {
     "nacl4096": {"workload": "nacl_rocksalt16_4096", "atoms": 4096, "density_g_cm3": 1.55, "T_K": 1200,
                  "dsf_alpha_per_A": 0.2, "dsf_rc_A": 12.0, "dt_fs": 1.0, "forces": "LennardJones+DampedShiftedCoulomb"},
     "argon864": {"workload": "argon_fcc6_864", "atoms": 864, "box_sigma": 10.229, "T_K": 94.4, "dt_fs": 10.0,
+                 "forces": "LennardJones"},
+    "ensemble": {"workload": "lj_ensemble_256x3", "replicas": 256, "trajectories": 768, "atoms": 6038184,
+                 "sizes": "log-uniform 256..32000 (fcc 4 nc^3, seed 0)", "rho_star": 0.8442, "T_star": 0.72,
+                 "cutoff_sigma": 2.5, "skin_sigma": 0.3, "dt_star": [0.005, 0.0025, 0.00125],
                  "forces": "LennardJones"},
 }
 

@@ -133,6 +133,10 @@ def timestep_convergence(sim, duration, start=None) -> Check:
     (accusim/accuracy.py:191-221)."""
     if sim.integrator.stochastic or sim.reactions:
         return Check("timestep error", NA, None, "stochastic run: compare ensemble statistics instead")
+    if start is None and hasattr(sim, "engine"):
+        # device-resident simulation: the three runs advance together as one batch of replicas
+        from .ensemble import timestep_check
+        return timestep_check(sim, duration)
     base = start or sim._initial
     T = si(duration, "s")
     n = max(int(round(T / sim.dt)), 1)

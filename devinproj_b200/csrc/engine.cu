@@ -423,6 +423,107 @@ __device__ int block_scan_excl(int v, int* total) {
   return ex;
 }
 
+// Per-atom state of the list build: stencil ranges, FP32 screen and the exact FP64 decision.
+struct PairScan {
+  const Eng& E;
+  const RepDev& R;
+  int64_t i;
+  int c[3], lo[3], hi[3];
+  bool one[3], any_one;
+  float4 pi;
+  float lo_f, hi_f, Lf[3];
+  const float4* im;
+  int32_t* lst;
+
+  __device__ PairScan(const Eng& e, const RepDev& r, int64_t atom, int dst) : E(e), R(r), i(atom) {
+    cell_coords(E.cellid[i] - R.cellbase, R, c[0], c[1], c[2]);
+    im = E.img[dst];
+    pi = im[i];
+    const float rl2f = (float)R.rl2;
+    lo_f = rl2f * (1.0f - 1e-4f);
+    hi_f = rl2f * (1.0f + 1e-4f);
+    any_one = false;
+    for (int d = 0; d < 3; ++d) {
+      Lf[d] = (float)R.L[d];
+      one[d] = R.nc[d] < 3;
+      any_one |= one[d];
+      lo[d] = one[d] ? 0 : -1;
+      hi[d] = one[d] ? 0 : 1;
+    }
+    lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
+  }
+  __device__ int cell(int a, int b, int d) const {
+    const int n0 = wrapc(c[0] + a, R.nc[0]), n1 = wrapc(c[1] + b, R.nc[1]), n2 = wrapc(c[2] + d, R.nc[2]);
+    return R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + n2;
+  }
+  __device__ static int scode(int a, int b, int d) { return (a + 1) + 3 * (b + 1) + 9 * (d + 1); }
+  // lower bound of the distance^2 from atom i to the neighbour cell's box, beyond the list radius?
+  __device__ bool cell_beyond(int a, int b, int d) const {
+    const float p[3] = {pi.x, pi.y, pi.z};
+    const int o[3] = {a, b, d};
+    float g2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (one[k] || o[k] == 0) continue;
+      const float gap = o[k] < 0 ? p[k] : R.csf[k] - p[k];
+      g2 += gap > 0.f ? gap * gap : 0.f;
+    }
+    return g2 > hi_f;
+  }
+  // FP32 r^2 of up to four consecutive candidates (stencil cells only; no per-axis wrap needed)
+  __device__ void screen4(int k, int k1, int a, int b, int d, float q[4]) const {
+    const float sa = a * R.csf[0], sb = b * R.csf[1], sd = d * R.csf[2];
+    float4 pj[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) pj[t] = im[min(k + t, k1 - 1)];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      float x = (pj[t].x - pi.x) + sa, y = (pj[t].y - pi.y) + sb, z = (pj[t].z - pi.z) + sd;
+      if (any_one) {
+        if (one[0]) x -= x > 0.5f * Lf[0] ? Lf[0] : (x < -0.5f * Lf[0] ? -Lf[0] : 0.f);
+        if (one[1]) y -= y > 0.5f * Lf[1] ? Lf[1] : (y < -0.5f * Lf[1] ? -Lf[1] : 0.f);
+        if (one[2]) z -= z > 0.5f * Lf[2] ? Lf[2] : (z < -0.5f * Lf[2] ? -Lf[2] : 0.f);
+      }
+      q[t] = x * x + y * y + z * z;
+    }
+  }
+  // Exact decision for candidate k: the code to store, or -1. Band candidates use the FP64 filter; others
+  // are decided by the FP32 screen (with the FP32 wrap for one-cell axes).
+  __device__ int test(int k, int a, int b, int d) const {
+    const float4 pj = im[k];
+    float x = (pj.x - pi.x) + a * R.csf[0], y = (pj.y - pi.y) + b * R.csf[1], z = (pj.z - pi.z) + d * R.csf[2];
+    int w[3] = {0, 0, 0};
+    if (one[0]) { w[0] = x > 0.5f * Lf[0] ? 1 : (x < -0.5f * Lf[0] ? -1 : 0); x -= w[0] * Lf[0]; }
+    if (one[1]) { w[1] = y > 0.5f * Lf[1] ? 1 : (y < -0.5f * Lf[1] ? -1 : 0); y -= w[1] * Lf[1]; }
+    if (one[2]) { w[2] = z > 0.5f * Lf[2] ? 1 : (z < -0.5f * Lf[2] ? -1 : 0); z -= w[2] * Lf[2]; }
+    const float q = x * x + y * y + z * z;
+    if (!(q < hi_f)) return -1;
+    if (q <= lo_f) {
+      const int mx = one[0] ? -w[0] : a, my = one[1] ? -w[1] : b, mz = one[2] ? -w[2] : d;
+      return (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+    }
+    double dx = sub(E.tmp_xa[3 * k], E.tmp_xa[3 * i]);
+    double dy = sub(E.tmp_xa[3 * k + 1], E.tmp_xa[3 * i + 1]);
+    double dz = sub(E.tmp_xa[3 * k + 2], E.tmp_xa[3 * i + 2]);
+    const int kx = dx > 0.5 * R.L[0] ? 1 : (dx < -0.5 * R.L[0] ? -1 : 0);
+    const int ky = dy > 0.5 * R.L[1] ? 1 : (dy < -0.5 * R.L[1] ? -1 : 0);
+    const int kz = dz > 0.5 * R.L[2] ? 1 : (dz < -0.5 * R.L[2] ? -1 : 0);
+    if (kx) dx = sub(dx, kx > 0 ? R.L[0] : -R.L[0]);
+    if (ky) dy = sub(dy, ky > 0 ? R.L[1] : -R.L[1]);
+    if (kz) dz = sub(dz, kz > 0 ? R.L[2] : -R.L[2]);
+    if (!(norm2(dx, dy, dz) < R.rl2)) return -1;
+    const int mx = one[0] ? -kx : a, my = one[1] ? -ky : b, mz = one[2] ? -kz : d;
+    return (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+  }
+  __device__ void finish(int cnt) const {
+    E.nnb[i] = min(cnt, E.maxnb);
+    if (cnt > E.maxnb) {
+      atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
+      atomicMax(&E.status->need_nbr, cnt);
+    }
+  }
+};
+
 // Rebuild of flagged replicas and per-replica record reduction. Cooperative launch (all blocks resident);
 // every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging.
 __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
@@ -632,112 +733,66 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   // pair set is exactly the FP64 filter's. That filter takes the minimum image by comparison with box/2,
   // which for every pair that can lie inside the list radius (< box/2) is the IEEE result of
   // d - box*round(d/box). The image shift stored with j is the stencil offset (>= 3 cells per edge) or
-  // minus the wrap (1 cell per edge).
-  {
-    const float4* __restrict__ im = E.img[dst];
-    const int G = E.G;
+  // minus the wrap (1 cell per edge). Entries are in stencil order, ascending slot within a cell, however
+  // the work is split: a warp per atom when the pair kernel runs >= 8 threads per atom (small systems),
+  // else a thread per atom that skips neighbour cells whose box lies beyond the list radius.
+  if (E.tpa >= 8) {
+    const int64_t gw = gtid >> 5, nw = gstride >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = gw; i < E.S; i += nw) {
+      const int r = E.tile_rep[i >> 5];
+      if (!fl[r]) continue;
+      const RepDev& R = E.rep[r];
+      if (i - R.atom0 >= R.n) continue;
+      PairScan ps(E, R, i, dst);
+      int cnt = 0;
+      for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
+        for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
+          for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
+            const int cc = ps.cell(a, b, d);
+            const int k0 = E.start[cc], k1 = E.start[cc + 1];
+            for (int base = k0; base < k1; base += 32) {
+              const int k = base + lane;
+              int code = -1;
+              if (k < k1 && k != i) code = ps.test(k, a, b, d);
+              const unsigned bal = __ballot_sync(0xffffffffu, code >= 0);
+              const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+              if (code >= 0 && pos < E.maxnb) ps.lst[(int64_t)pos * E.G] = (int32_t)((uint32_t)k | ((uint32_t)code << kIdxBits));
+              cnt += __popc(bal);
+            }
+          }
+      if (lane == 0) ps.finish(cnt);
+    }
+  } else {
     for (int64_t i = gtid; i < E.S; i += gstride) {
       const int r = E.tile_rep[i >> 5];
       if (!fl[r]) continue;
       const RepDev& R = E.rep[r];
       if (i - R.atom0 >= R.n) continue;
-      int c0, c1, c2;
-      cell_coords(E.cellid[i] - R.cellbase, R, c0, c1, c2);
-      const float4 pi = im[i];
-      const float rl2f = (float)R.rl2;
-      const float lo_f = rl2f * (1.0f - 1e-4f), hi_f = rl2f * (1.0f + 1e-4f);
-      const float Lf0 = (float)R.L[0], Lf1 = (float)R.L[1], Lf2 = (float)R.L[2];
-      const bool one0 = R.nc[0] < 3, one1 = R.nc[1] < 3, one2 = R.nc[2] < 3;
-      const bool any_one = one0 || one1 || one2;
-      int lo0, hi0, lo1, hi1, lo2, hi2;
-      stencil(c0, R.nc[0], lo0, hi0);
-      stencil(c1, R.nc[1], lo1, hi1);
-      stencil(c2, R.nc[2], lo2, hi2);
-      int32_t* lst = E.nbr + (i / G) * (int64_t)E.maxnb * G + (i % G);
+      PairScan ps(E, R, i, dst);
       int cnt = 0;
-      // exact decision for a band candidate k; returns the code or -1
-      auto exact = [&](int k, int a, int b, int d) -> int {
-        double dx = sub(E.tmp_xa[3 * k], E.tmp_xa[3 * i]);
-        double dy = sub(E.tmp_xa[3 * k + 1], E.tmp_xa[3 * i + 1]);
-        double dz = sub(E.tmp_xa[3 * k + 2], E.tmp_xa[3 * i + 2]);
-        const int kx = dx > 0.5 * R.L[0] ? 1 : (dx < -0.5 * R.L[0] ? -1 : 0);
-        const int ky = dy > 0.5 * R.L[1] ? 1 : (dy < -0.5 * R.L[1] ? -1 : 0);
-        const int kz = dz > 0.5 * R.L[2] ? 1 : (dz < -0.5 * R.L[2] ? -1 : 0);
-        if (kx) dx = sub(dx, kx > 0 ? R.L[0] : -R.L[0]);
-        if (ky) dy = sub(dy, ky > 0 ? R.L[1] : -R.L[1]);
-        if (kz) dz = sub(dz, kz > 0 ? R.L[2] : -R.L[2]);
-        if (!(norm2(dx, dy, dz) < R.rl2)) return -1;
-        const int mx = one0 ? -kx : a, my = one1 ? -ky : b, mz = one2 ? -kz : d;
-        return (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
-      };
-      auto keep = [&](int k, int code) {
-        if (cnt < E.maxnb) lst[(int64_t)cnt * G] = (int32_t)((uint32_t)k | ((uint32_t)code << kIdxBits));
-        ++cnt;
-      };
-      for (int a = lo0; a <= hi0; ++a) {
-        const int n0 = wrapc(c0 + a, R.nc[0]);
-        const float sa = a * R.csf[0];
-        for (int b = lo1; b <= hi1; ++b) {
-          const int n1 = wrapc(c1 + b, R.nc[1]);
-          const float sb = b * R.csf[1];
-          for (int d = lo2; d <= hi2; ++d) {
-            const float sd = d * R.csf[2];
-            const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + wrapc(c2 + d, R.nc[2]);
+      for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
+        for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
+          for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
+            if (ps.cell_beyond(a, b, d)) continue;
+            const int cc = ps.cell(a, b, d);
             const int k0 = E.start[cc], k1 = E.start[cc + 1];
-            const int scode = (a + 1) + 3 * (b + 1) + 9 * (d + 1);
-            if (!any_one) {
-              int k = k0;
-              for (; k + 2 <= k1; k += 2) {
-                const float4 pj0 = im[k], pj1 = im[k + 1];
-                const float x0 = (pj0.x - pi.x) + sa, y0 = (pj0.y - pi.y) + sb, z0 = (pj0.z - pi.z) + sd;
-                const float x1 = (pj1.x - pi.x) + sa, y1 = (pj1.y - pi.y) + sb, z1 = (pj1.z - pi.z) + sd;
-                const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
-                if (k != i && q0 < hi_f) {
-                  const int c = q0 <= lo_f ? scode : exact(k, a, b, d);
-                  if (c >= 0) keep(k, c);
-                }
-                if (k + 1 != i && q1 < hi_f) {
-                  const int c = q1 <= lo_f ? scode : exact(k + 1, a, b, d);
-                  if (c >= 0) keep(k + 1, c);
-                }
-              }
-              if (k < k1 && k != i) {
-                const float4 pj = im[k];
-                const float x = (pj.x - pi.x) + sa, y = (pj.y - pi.y) + sb, z = (pj.z - pi.z) + sd;
-                const float q = x * x + y * y + z * z;
-                if (q < hi_f) {
-                  const int c = q <= lo_f ? scode : exact(k, a, b, d);
-                  if (c >= 0) keep(k, c);
-                }
-              }
-            } else {
-              for (int k = k0; k < k1; ++k) {
-                if (k == i) continue;
-                const float4 pj = im[k];
-                float fx = (pj.x - pi.x) + sa, fy = (pj.y - pi.y) + sb, fz = (pj.z - pi.z) + sd;
-                int wx = 0, wy = 0, wz = 0;
-                if (one0) wx = fx > 0.5f * Lf0 ? 1 : (fx < -0.5f * Lf0 ? -1 : 0);
-                if (one1) wy = fy > 0.5f * Lf1 ? 1 : (fy < -0.5f * Lf1 ? -1 : 0);
-                if (one2) wz = fz > 0.5f * Lf2 ? 1 : (fz < -0.5f * Lf2 ? -1 : 0);
-                fx -= wx * Lf0;
-                fy -= wy * Lf1;
-                fz -= wz * Lf2;
-                const float q = fx * fx + fy * fy + fz * fz;
-                if (q < hi_f) {
-                  const int mx = one0 ? -wx : a, my = one1 ? -wy : b, mz = one2 ? -wz : d;
-                  const int c = q <= lo_f ? (mx + 1) + 3 * (my + 1) + 9 * (mz + 1) : exact(k, a, b, d);
-                  if (c >= 0) keep(k, c);
+            for (int k = k0; k < k1; k += 4) {
+              float q[4];
+              ps.screen4(k, k1, a, b, d, q);
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                if (k + t < k1 && k + t != i && q[t] < ps.hi_f) {
+                  const int code = q[t] <= ps.lo_f && !ps.any_one ? ps.scode(a, b, d) : ps.test(k + t, a, b, d);
+                  if (code >= 0) {
+                    if (cnt < E.maxnb) ps.lst[(int64_t)cnt * E.G] = (int32_t)((uint32_t)(k + t) | ((uint32_t)code << kIdxBits));
+                    ++cnt;
+                  }
                 }
               }
             }
           }
-        }
-      }
-      E.nnb[i] = min(cnt, E.maxnb);
-      if (cnt > E.maxnb) {
-        atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
-        atomicMax(&E.status->need_nbr, cnt);
-      }
+      ps.finish(cnt);
     }
   }
   __syncthreads();

@@ -306,6 +306,9 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=
         if s.dim != 3 or not s.periodic:
             raise ValueError("the engine runs 3-dimensional periodic systems")
     species = systems[0].species
+    if tpa == "auto":
+        from .autotune import tune
+        tpa, grid_mult = tune(systems, forces, dts)
     reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
     for attempt in range(3):
         eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,

@@ -141,3 +141,34 @@ def test_engine_rejects_unsupported_setups():
     s3.add("Na", [[0, 0, 0], [2e-10, 0, 0]])
     with pytest.raises(ValueError):
         GpuSimulation(s3, [DampedShiftedCoulomb(rcut=1e-9, exclude=[(0, 1)])], dt=1e-15)
+
+
+@pytest.mark.parametrize("seed", [0, 5])
+def test_list_build_variants_agree(seed):
+    """The warp-per-atom list build (>= 8 threads per atom) and the culled thread-per-atom build produce the
+    same pair sets; both give FP64-oracle forces."""
+    from devinproj_b200 import configs
+    from devinproj_b200.engine import ACC, LEN, start_engine
+    s, lj = configs.lj_fluid(6, seed=seed)
+    s.maxwell_boltzmann(250.0, np.random.default_rng(seed))
+    out = {}
+    for tpa in (1, 8):
+        eng, _, _ = start_engine([s], [lj], [0.005 * configs.AR_TAU], tpa=tpa)
+        eng.run(40, 0, True)   # several rebuilds
+        mx, total = eng.neighbor_stats()
+        pairs = eng.count_pairs()
+        p, v, a = eng.get_state()
+        out[tpa] = (total, pairs, p.cpu().numpy() * LEN, a.cpu().numpy() * ACC, eng.status().rebuilds)
+    assert out[1][4] > 1 and out[8][4] > 1
+    for tpa in (1, 8):
+        st = port.State(out[tpa][2], np.zeros_like(out[tpa][2]), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                        [("Ar", configs.AR_MASS, 0.0)])
+        Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(st)
+        assert rms_rel(out[tpa][3] * configs.AR_MASS, Fo) <= 1e-5
+    # fresh engines on identical positions: identical list totals and pair counts
+    s.pos = out[1][2]
+    totals = []
+    for tpa in (1, 8):
+        eng, _, _ = start_engine([s], [lj], [0.005 * configs.AR_TAU], tpa=tpa)
+        totals.append((eng.neighbor_stats()[1], eng.count_pairs()))
+    assert totals[0] == totals[1]
