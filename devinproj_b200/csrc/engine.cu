@@ -25,6 +25,8 @@
 #include <vector>
 
 #include "accusim_b200_engine.h"
+#include "accusim_b200_mlp.h"
+#include <cuda_bf16.h>
 #include "common.cuh"
 
 using namespace acs;
@@ -90,6 +92,7 @@ struct Eng {
   acs_dev_status* status;
   unsigned int* bar;  // [0] counter, [1] generation
   unsigned long long* phase_ns;  // rebuild phase durations, accumulated (block 0 timestamps)
+  const float* fext;             // optional per-slot force added to the pair forces (learned correction)
 };
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -300,6 +303,11 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
       if (REC) deu += __shfl_xor_sync(0xffffffffu, deu, off);
     }
     if (valid && phase == 0) {
+      if (E.fext) {
+        dfx += (double)E.fext[3 * i];
+        dfy += (double)E.fext[3 * i + 1];
+        dfz += (double)E.fext[3 * i + 2];
+      }
       const double im = ff.inv_mass[si];
       const double ax = dfx * im, ay = dfy * im, az = dfz * im;
       if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(&E.status->flags, ACS_FLAG_NONFINITE);
@@ -899,6 +907,69 @@ __global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out)
   atomicAdd(out + 1, nd);
 }
 
+// Radial descriptors of every slot from the engine's own images and neighbour lists (FP32), in slot order,
+// for the learned force correction: warp per slot, lane = Gaussian channel (definitions as in mlp.cu).
+struct DescP {
+  float r0, dmu, inv2s2, rc2, pi_rc;
+};
+
+__global__ void __launch_bounds__(256) k_desc_engine(Eng E, int src, DescP P, const float* __restrict__ mean,
+                                                      const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ X,
+                                                      float* __restrict__ V) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= E.S) return;
+  const int r = E.tile_rep[i >> 5];
+  const RepDev& R = E.rep[r];
+  const bool valid = E.active[r] && (i - R.atom0 < R.n);
+  float d[2] = {0.f, 0.f}, vx[2] = {0.f, 0.f}, vy[2] = {0.f, 0.f}, vz[2] = {0.f, 0.f};
+  int si = 0;
+  if (valid) {
+    const float4* __restrict__ im = E.img[src];
+    const float4 pi = im[i];
+    si = __float_as_int(pi.w);
+    const float mu = P.r0 + lane * P.dmu;
+    const int m = E.nnb[i];
+    const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
+    for (int k = 0; k < m; ++k) {
+      const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
+      const float4 pj = im[e & kIdxMask];
+      const uint32_t code = e >> kIdxBits;
+      const float fx = (pj.x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
+      const float fy = (pj.y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
+      const float fz = (pj.z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
+      const float r2 = fx * fx + fy * fy + fz * fz;
+      if (!(r2 < P.rc2)) continue;
+      const float rr = sqrtf(r2);
+      const float fc = 0.5f * (__cosf(P.pi_rc * rr) + 1.0f);
+      const float t = rr - mu;
+      const float g = __expf(-t * t * P.inv2s2) * fc;
+      const float gr = g / rr;
+      const int s = __float_as_int(pj.w) & 1;
+      d[s] += g;
+      vx[s] += gr * fx;
+      vy[s] += gr * fy;
+      vz[s] += gr * fz;
+    }
+  }
+  __nv_bfloat16* xrow = X + i * 80;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int c = 32 * s + lane;
+    xrow[c] = __float2bfloat16(valid ? (d[s] - mean[c]) * inv_std[c] : 0.f);
+    float* vrow = V + (i * 64 + c) * 3;
+    vrow[0] = vx[s];
+    vrow[1] = vy[s];
+    vrow[2] = vz[s];
+  }
+  if (lane < 16) {
+    float v = 0.f;
+    if (valid && lane < 2) v = (si == lane) ? 1.f : 0.f;
+    if (valid && lane == 15) v = 1.f;
+    xrow[64 + lane] = __float2bfloat16(v);
+  }
+}
+
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
@@ -916,6 +987,17 @@ struct acs_engine {
   int n_lj = 0, n_dsf = 0;
   std::map<long long, cudaGraphExec_t> graphs;
   int dev = 0;
+  // learned force correction (optional)
+  bool corr = false;
+  DescP dp{};
+  const float *c_mean = nullptr, *c_inv_std = nullptr, *c_b2 = nullptr, *c_b3 = nullptr;
+  const void* c_w5[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float c_scale = 1.f;
+  void* c_X = nullptr;
+  float* c_V = nullptr;
+  float* c_F = nullptr;
+  int32_t* c_status = nullptr;
+  float last_corr_ms = 0.f;
 };
 
 namespace {
@@ -1129,6 +1211,17 @@ int launch_step(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t
              : launch_step_t<false, true, false>(e, rec, mode, src, dst, s);
 }
 
+// Descriptors + tensor-core MLP -> per-slot correction forces for the images in buffer `src`.
+int launch_correction(acs_engine* e, int src, cudaStream_t s) {
+  if (!e->corr) return ACS_OK;
+  const int64_t threads = e->E.S * 32;
+  k_desc_engine<<<(int)((threads + 255) / 256), 256, 0, s>>>(e->E, src, e->dp, e->c_mean, e->c_inv_std,
+                                                              (__nv_bfloat16*)e->c_X, e->c_V);
+  int st = launch_status();
+  if (st) return st;
+  return acs_mlp_forward(e->c_X, e->c_V, e->E.S, e->c_w5, e->c_b2, e->c_b3, e->c_scale, e->c_F, e->c_status, s);
+}
+
 int launch_rebuild(acs_engine* e, int dst, int rec, int rec_idx, int force_all, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(e->coop_blocks);
@@ -1156,6 +1249,7 @@ int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cud
     const int src = k & 1, dst = (k + 1) & 1;
     const bool last = (k == steps - 1);
     const int rec = rec_at[k] ? 1 : 0;
+    if ((st = launch_correction(e, src, s))) return st;
     if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, s))) return st;
     if (!last || rec) {
       if ((st = launch_rebuild(e, dst, rec, rec_idx, 0, s))) return st;
@@ -1329,6 +1423,7 @@ int acs_engine_set_state(acs_engine* e, const double* pos, const double* vel, co
   if (st) return st;
   // build lists for every replica, then one force evaluation (accelerations + initial records)
   if ((st = launch_rebuild(e, 0, 0, 0, 1, s))) return st;
+  if ((st = launch_correction(e, 0, s))) return st;
   if ((st = launch_step(e, 1, 2, 0, 0, s))) return st;
   return launch_rebuild(e, 0, 1, 0, 0, s);
 }
@@ -1458,7 +1553,7 @@ int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* str
 int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, float* out_ms, void* stream) {
   if (!e || steps < 1 || !out_ms) return ACS_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<cudaEvent_t> ev(4 * (size_t)steps + 4);
+  std::vector<cudaEvent_t> ev(6 * (size_t)steps + 4);
   for (auto& x : ev)
     if (cudaEventCreate(&x) != cudaSuccess) return ACS_ERR_CUDA;
   int st = ACS_OK;
@@ -1480,13 +1575,14 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
     const int src = k & 1, dst = (k + 1) & 1;
     const bool last = (k == steps - 1);
     const int rec = ((record_every > 0 && (k + 1) % record_every == 0) || last) ? 1 : 0;
-    st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, s); });
+    if (e->corr) st = mark(2, [&] { return launch_correction(e, src, s); });
+    if (!st) st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, s); });
     if (!st) st = mark(1, [&] { return launch_rebuild(e, dst, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, 0, s); });
     rec_idx += rec;
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) st = ACS_ERR_CUDA;
-  float tot[2] = {0.f, 0.f};
-  int cnt[2] = {0, 0};
+  float tot[3] = {0.f, 0.f, 0.f};
+  int cnt[3] = {0, 0, 0};
   for (auto& sp : spans) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ev[sp.first], ev[sp.first + 1]) == cudaSuccess) {
@@ -1499,6 +1595,7 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
   out_ms[1] = tot[1];
   out_ms[2] = (float)cnt[0];
   out_ms[3] = (float)cnt[1];
+  e->last_corr_ms = cnt[2] ? tot[2] / cnt[2] : 0.f;
   return st;
 }
 
@@ -1508,6 +1605,37 @@ int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear) 
   if (clear && cudaMemset(e->E.phase_ns, 0, 8 * 16) != cudaSuccess) return ACS_ERR_CUDA;
   return ACS_OK;
 }
+
+int acs_engine_set_correction(acs_engine* e, const float* params6, const float* mean, const float* inv_std,
+                              const void* const* w5, const float* b2, const float* b3, float out_scale, void* X,
+                              float* V, float* F, int32_t* status_dev, int enabled) {
+  if (!e) return ACS_ERR_ARG;
+  if (enabled && (!params6 || !mean || !inv_std || !w5 || !b2 || !b3 || !X || !V || !F || !status_dev))
+    return ACS_ERR_ARG;
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  e->graphs.clear();
+  e->corr = enabled != 0;
+  e->E.fext = e->corr ? F : nullptr;
+  if (!e->corr) return ACS_OK;
+  e->dp.r0 = params6[0];
+  e->dp.dmu = params6[1];
+  e->dp.inv2s2 = params6[2];
+  e->dp.rc2 = params6[3] * params6[3];
+  e->dp.pi_rc = (float)M_PI / params6[3];
+  e->c_mean = mean;
+  e->c_inv_std = inv_std;
+  for (int k = 0; k < 5; ++k) e->c_w5[k] = w5[k];
+  e->c_b2 = b2;
+  e->c_b3 = b3;
+  e->c_scale = out_scale;
+  e->c_X = X;
+  e->c_V = V;
+  e->c_F = F;
+  e->c_status = status_dev;
+  return ACS_OK;
+}
+
+float acs_engine_last_correction_ms(acs_engine* e) { return e ? e->last_corr_ms : 0.f; }
 
 int acs_engine_destroy(acs_engine* e) {
   if (!e) return ACS_OK;

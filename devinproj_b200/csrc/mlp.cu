@@ -478,8 +478,15 @@ int acs_mlp_forward(const void* X, const float* V, int64_t n, const void* const*
                     float out_scale, float* F, int32_t* status_dev, void* stream) {
   if (n < 1 || !X || !V || !w5 || !b2 || !b3 || !F || !status_dev) return ACS_ERR_ARG;
   const size_t smem = MlpSmem::END;
-  if (cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return ACS_ERR_CUDA;
+  // set once per device: this launch may sit inside a CUDA graph capture
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ACS_ERR_NO_DEVICE;
+  if (!attr_set[dev]) {
+    if (cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return ACS_ERR_CUDA;
+    attr_set[dev] = true;
+  }
   MlpWeights W{(const bf16*)w5[0], (const bf16*)w5[1], (const bf16*)w5[2], (const bf16*)w5[3], (const bf16*)w5[4], b2, b3};
   k_mlp<false><<<(int)ceil_div(n, kTile), 128, smem, (cudaStream_t)stream>>>((const bf16*)X, V, nullptr, n, W, out_scale,
                                                                             0.f, F, nullptr, nullptr, status_dev);

@@ -70,6 +70,8 @@ ENGINE_SIGNATURES = {
     "acs_engine_count_pairs": (C.c_int, [P, P, P]),
     "acs_engine_run_timed": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(C.c_float), P]),
     "acs_engine_phase_times": (C.c_int, [P, P, C.c_int]),
+    "acs_engine_set_correction": (C.c_int, [P, P, P, P, P, P, P, C.c_float, P, P, P, P, C.c_int]),
+    "acs_engine_last_correction_ms": (C.c_float, [P]),
     "acs_engine_destroy": (C.c_int, [P]),
 }
 _lib.SIGNATURES.update(ENGINE_SIGNATURES)
@@ -159,6 +161,8 @@ class Engine:
                    "acs_engine_create")
         self.maxnb = int(maxnb)
         self.rec_cap = int(rec_cap)
+        self.rlist_engine = float(replicas[0]["rlist"])
+        self.correction = None
         self.counts = np.array([int(r["n"]) for r in replicas])
         self.offsets = np.concatenate([[0], np.cumsum(self.counts)])
         self._rec_buf = torch.empty(rec_cap * self.R * 8, dtype=torch.float64, device="cuda")
@@ -205,6 +209,29 @@ class Engine:
     def run(self, steps: int, record_every: int = 0, record_last: bool = True):
         _lib.check(self.L.acs_engine_run(self.h, int(steps), int(record_every), 1 if record_last else 0,
                                          stream_handle()), "acs_engine_run")
+
+    def set_correction(self, lc, enabled=True):
+        """Attach (or detach) a LearnedCorrection: evaluated inside every force evaluation of later runs."""
+        if not enabled or lc is None:
+            _lib.check(self.L.acs_engine_set_correction(self.h, None, None, None, None, None, None, 0.0, None, None,
+                                                        None, None, 0), "acs_engine_set_correction")
+            self.correction = None
+            return
+        S = self.launch_info()[2]
+        if lc.desc.p["rc"] > self.rlist_engine:
+            raise ValueError("descriptor radius exceeds the engine's neighbour-list radius")
+        self._cX = torch.zeros((S, 80), dtype=torch.bfloat16, device="cuda")
+        self._cV = torch.zeros((S, 64, 3), dtype=torch.float32, device="cuda")
+        self._cF = torch.zeros((S, 3), dtype=torch.float32, device="cuda")
+        m = lc.mlp
+        _lib.check(self.L.acs_engine_set_correction(self.h, lc.desc.params6.ctypes.data, lc.desc.mean.data_ptr(),
+                                                    lc.desc.inv_std.data_ptr(), m._w5, m.b2.data_ptr(), m.b3.data_ptr(),
+                                                    float(lc.scale), self._cX.data_ptr(), self._cV.data_ptr(),
+                                                    self._cF.data_ptr(), m.status.ptr, 1), "acs_engine_set_correction")
+        self.correction = lc
+
+    def last_correction_ms(self):
+        return float(self.L.acs_engine_last_correction_ms(self.h))
 
     def run_timed(self, steps: int, record_every: int = 0):
         """Eager launches of one block with per-kernel CUDA events: (step ms avg, rebuild ms avg, total ms)."""
@@ -335,7 +362,7 @@ class GpuSimulation:
     `run` call (and at records when positions=True)."""
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
-                 rec_cap=256, grid_mult=0, tpa=None):
+                 rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500):
         from .integrators import VelocityVerlet
         from .simulation import Trajectory
         from .units import si
@@ -357,8 +384,35 @@ class GpuSimulation:
         self.engine, self.rlist, self.half_skin = start_engine(
             [system], self.forces, [self.dt if self.dt is not None else 1e-15], maxnb=maxnb, rec_cap=rec_cap,
             grid_mult=grid_mult, tpa=tpa)
+        self.correction = None
+        self.validate_every = int(validate_every)
+        self.validations = []
+        if correction is not None:
+            self.set_correction(correction)
         self._last = self.engine.records(1)[0, 0]
         self._pull()
+
+    def set_correction(self, lc, enabled=True):
+        """Add a trained LearnedCorrection to the DSF forces (re-evaluates the current forces)."""
+        self.engine.set_correction(lc, enabled)
+        self.correction = lc if enabled else None
+        _upload_state(self.engine, [self.system])
+        self.engine.check("set_correction")
+        self._last = self.engine.records(1)[0, 0]
+        self._pull()
+
+    def validate(self):
+        """Judge the corrected electrostatic forces against the device Ewald on the current state; switch the
+        correction off (fallback to plain DSF) unless it improves on DSF. Returns (err_dsf, err_corrected)."""
+        from .ewald import Ewald
+        dsf = [f for f in self.forces if type(f).__name__ == "DampedShiftedCoulomb"][0]
+        Fd, _ = dsf.compute(self.system)
+        Fe, _ = Ewald(k=dsf.k).compute(self.system)
+        e0, e1, on = self.correction.validate(self.system, Fd, Fe)
+        self.validations.append((self.steps, e0, e1, on))
+        if not on:
+            self.set_correction(None, enabled=False)
+        return e0, e1
 
     # state ------------------------------------------------------------------------------------------
     def _pull(self):
@@ -410,23 +464,25 @@ class GpuSimulation:
         done = 0
         while done < steps:
             left = steps - done
-            if positions:
-                block = min(re, left)
+            if self.correction is not None and self.validate_every > 0:
+                left = min(left, self.validate_every - self.steps % self.validate_every)
+            off = done % re
+            if positions or off:
+                block = min(re - off, left)       # up to the next record step
             else:
-                span = re * max(1, min(eng.rec_cap - 1, 4000 // re))
-                block = min(span, left)
-            end_of_run = block == left
-            periodic = 0 if positions else re
-            eng.run(block, periodic, end_of_run or positions)
-            marks = [] if positions else list(range(re, block + 1, re))
-            if (end_of_run or positions) and (not marks or marks[-1] != block):
-                marks.append(block)
-            recs = eng.records(len(marks))[:, 0, :]
+                block = min(re * max(1, min(eng.rec_cap - 1, 4000 // re)), left)
+            periodic = 0 if (positions or off) else re
+            eng.run(block, periodic, True)        # every block also records its last step
+            local = list(range(periodic, block + 1, periodic)) if periodic else []
+            if not local or local[-1] != block:
+                local.append(block)
+            recs = eng.records(len(local))[:, 0, :]
             eng.check("engine run")
-            if positions:
+            kept = [(j, rec) for j, rec in zip(local, recs) if (done + j) % re == 0 or done + j == steps]
+            if positions and kept:
                 self._pull_positions()
             j0 = 0
-            for j, rec in zip(marks, recs):
+            for j, rec in kept:
                 for _ in range(j - j0):
                     self.time += self.dt
                 j0 = j
@@ -436,6 +492,9 @@ class GpuSimulation:
             self._last = recs[-1]
             self.steps += block
             done += block
+            if self.correction is not None and self.validate_every > 0 and self.steps % self.validate_every == 0:
+                self._pull()
+                self.validate()
         self._pull()
         return self.trajectory
 

@@ -85,6 +85,16 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
  * [1] flag read, [2] clear, [3] bin, [4..6] scan, [7] scatter, [8] in-cell sort, [9] gather, [10] commit,
  * [15] list build (block 0 share). Synchronous. */
 int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear);
+/* Learned force correction (no counterpart in the reference): when enabled, every force evaluation first
+ * computes the radial descriptors of all slots from the engine's images and lists (radius params6[3] <= list
+ * radius) into X (S x 80 BF16) and V (S x 64 x 3 FP32), runs the tensor-core MLP (acs_mlp_forward) into
+ * F (S x 3 FP32, slot order, engine force units) and adds F to the pair forces. Buffers are caller-owned
+ * (S = acs_engine_launch_info's slots). Changing it drops the cached graphs. */
+int acs_engine_set_correction(acs_engine* e, const float* params6, const float* mean, const float* inv_std,
+                              const void* const* w5, const float* b2, const float* b3, float out_scale, void* X,
+                              float* V, float* F, int32_t* status_dev, int enabled);
+/* Mean duration (ms) of the correction launches in the last acs_engine_run_timed call. */
+float acs_engine_last_correction_ms(acs_engine* e);
 int acs_engine_destroy(acs_engine* e);
 
 #ifdef __cplusplus

@@ -142,3 +142,34 @@ def test_learned_correction_beats_plain_dsf_on_held_out_melt():
     s = lc._system(d, 39)
     _, _, on = lc.validate(s, d["dsf"][39], d["dsf"][39] + d["residual"][39])
     assert on
+
+
+def test_engine_runs_learned_correction_inside_the_step_loop():
+    """The correction evaluated inside the engine's graph equals the stand-alone prediction on the same state,
+    the Ewald validation runs every `validate_every` steps, and a correction that makes forces worse is
+    switched off (fallback to plain DSF)."""
+    from devinproj_b200 import GpuSimulation, configs
+    from devinproj_b200.engine import ACC
+    from devinproj_b200.learned import LearnedCorrection, generate_dataset, rms_rel
+    d = generate_dataset(12, seed=4, n_sites=8, melt_steps=800, equil_steps=200, interval=20)
+    lc = LearnedCorrection(seed=1)
+    lc.train(d, np.arange(10), epochs=30, batch_tiles=4, lr=3e-3)
+    s, forces = configs.nacl_melt(8, T=1300.0, rcut=10e-10, seed=4)
+    s.pos = d["pos"][11].copy()
+    sim = GpuSimulation(s, forces, dt=1e-15, correction=lc, validate_every=50)
+    plain = GpuSimulation(s.copy(), forces, dt=1e-15)
+    F_corr = lc.predict(s)
+    m = s.masses[:, None]
+    assert rms_rel(sim.force - plain.force, F_corr) <= 2e-2
+    sim.run(steps=120, record_every=10, positions=False)
+    assert [v[0] for v in sim.validations] == [50, 100]
+    assert len(sim.trajectory.t) == 13
+    # an untrained network (large random output) is worse than plain DSF: validation turns it off
+    bad = LearnedCorrection(seed=2)
+    bad.desc = lc.desc
+    bad.scale = 50.0 * lc.scale
+    sim2 = GpuSimulation(s.copy(), forces, dt=1e-15, correction=bad, validate_every=20)
+    sim2.run(steps=40, record_every=20, positions=False)
+    assert sim2.validations[0][3] is False and sim2.correction is None
+    assert np.all(np.isfinite(sim2.system.pos))
+    del m, ACC
