@@ -198,6 +198,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
+    ap.add_argument("--experiment", choices=["learned", "drift", "dropin"], default=None,
+                    help="accuracy experiments (one JSON line each): the learned DSF->Ewald correction at full scale, "
+                         "the 1e4-step energy drift of the 1M-atom run, the plain FP64 drop-in's throughput")
+    ap.add_argument("--snapshots", type=int, default=2000)
     ap.add_argument("--profile", action="store_true",
                     help="engine only: warm-up graph steps then --steps eager launches (for ncu), no timing legs")
     args = ap.parse_args()
@@ -212,6 +216,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             reference_arm(args, full_config(workload_meta(args.workload), args, world))
+        return
+    if args.experiment:
+        run_experiment(args)
         return
 
     import numpy as np
@@ -419,6 +426,100 @@ WORKLOADS = {
                  "cutoff_sigma": 2.5, "skin_sigma": 0.3, "dt_star": [0.005, 0.0025, 0.00125],
                  "forces": "LennardJones"},
 }
+
+
+def run_experiment(args):
+    """Accuracy experiments that back the design document's claims; each prints one JSON line."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(0)
+    if args.experiment == "learned":
+        from devinproj_b200 import GpuSimulation, configs
+        from devinproj_b200.learned import LearnedCorrection, generate_dataset
+        t0 = time.perf_counter()
+        d = generate_dataset(args.snapshots, seed=0, n_sites=20, verbose=False)
+        t_gen = time.perf_counter() - t0
+        n_train = int(0.9 * args.snapshots)
+        lc = LearnedCorrection(seed=0)
+        t0 = time.perf_counter()
+        hist = lc.train(d, np.arange(n_train), epochs=20, batch_tiles=64, lr=2e-3)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        e0, e1 = lc.errors(d, np.arange(n_train, args.snapshots))
+        # step-time overhead of the correction on the 8000-ion melt (eager per-kernel timing)
+        s, forces, dt = configs.nacl8000()
+        s.pos = d["pos"][-1].copy()
+        plain = GpuSimulation(s.copy(), forces, dt=dt)
+        plain.engine.run(20, 0, True)
+        k0, r0, t_plain = plain.engine.run_timed(200, 0)
+        corr = GpuSimulation(s.copy(), forces, dt=dt, correction=lc, validate_every=0)
+        corr.engine.run(20, 0, True)
+        k1, r1, t_c = corr.engine.run_timed(200, 0)
+        c_ms = corr.engine.last_correction_ms()
+        step_plain = t_plain / 200
+        step_corr = step_plain + c_ms
+        stride = 10
+        corr.engine.set_correction_stride(stride)
+        corr.engine.run(20, 0, True)
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record()
+        corr.engine.run(200, 0, True)
+        e_b.record()
+        plain_a, plain_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        plain.engine.run(200, 0, True)
+        torch.cuda.synchronize()
+        plain_a.record()
+        plain.engine.run(200, 0, True)
+        plain_b.record()
+        torch.cuda.synchronize()
+        graph_corr = e_a.elapsed_time(e_b) / 200
+        graph_plain = plain_a.elapsed_time(plain_b) / 200
+        print(json.dumps({"experiment": "learned_dsf_correction", "ions": 8000, "snapshots": args.snapshots,
+                          "train_snapshots": n_train, "dataset_s": t_gen, "train_s": t_train,
+                          "train_loss_first_last": [hist[0], hist[-1]],
+                          "heldout_rms_rel_err_dsf": e0, "heldout_rms_rel_err_corrected": e1, "error_ratio": e0 / e1,
+                          "step_ms_plain": step_plain, "correction_ms": c_ms,
+                          "overhead_frac": c_ms / step_plain, "step_ms_corrected": step_corr,
+                          "graph_ms_per_step_plain": graph_plain, "graph_ms_per_step_corrected_stride10": graph_corr,
+                          "overhead_frac_stride10": graph_corr / graph_plain - 1.0}), flush=True)
+    elif args.experiment == "drift":
+        from devinproj_b200.engine import start_engine
+        s, forces, dt, cfg = workload("lj1m", seed=0)
+        eng, _, _ = start_engine([s], forces, [dt], rec_cap=128)
+        steps, every = 10000, 100
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.run(steps, every, True)
+        e1.record()
+        torch.cuda.synchronize()
+        eng.check("drift run")
+        rec = eng.records(steps // every)[:, 0, :]
+        init = None
+        E = rec[:, 0] + rec[:, 1]
+        scale = max(abs(E[0]), np.max(np.abs(rec[:, 0])), np.max(np.abs(rec[:, 1])))
+        drift = float(np.max(np.abs(E - E[0])) / scale)
+        slope = float(np.polyfit(np.arange(len(E)) * every, E, 1)[0]) / scale
+        del init
+        print(json.dumps({"experiment": "energy_drift_lj1m", "steps": steps, "record_every": every,
+                          "energy_drift_report_metric": drift, "linear_drift_per_step_rel": slope,
+                          "ms_per_step": e0.elapsed_time(e1) / steps, "rebuilds": eng.status().rebuilds}), flush=True)
+    elif args.experiment == "dropin":
+        from devinproj_b200 import Simulation, VelocityVerlet
+        s, forces, dt, cfg = workload(args.workload, seed=0)
+        sim = Simulation(s, forces, integrator=VelocityVerlet(), dt=dt)
+        sim.run(steps=2, record_every=10 ** 9, positions=False)
+        torch.cuda.synchronize()
+        n = 5
+        t0 = time.perf_counter()
+        sim.run(steps=n, record_every=10 ** 9, positions=False)
+        torch.cuda.synchronize()
+        dt_s = time.perf_counter() - t0
+        print(json.dumps({"experiment": "fp64_dropin_throughput", "workload": cfg["workload"], "steps": n,
+                          "atom_steps_per_s": s.n * n / dt_s, "ms_per_step": 1e3 * dt_s / n,
+                          "path": "Simulation.run with the FP64 drop-in VelocityVerlet and forces (host state, "
+                                  "per-step H2D/D2H)"}), flush=True)
 
 
 def workload_meta(name):

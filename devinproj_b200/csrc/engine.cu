@@ -118,6 +118,22 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
   s = t;
 }
 
+// Kahan step for a product term a*b: the product enters the compensated sum through one FMA
+// (y = a*b - c rounded once), so the pair force is never rounded on its own.
+__device__ __forceinline__ void kahan_fma(float& s, float& c, float a, float b) {
+  const float y = fmaf(a, b, -c);
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// 1/x by the hardware approximation (relative error within 2^-22), one instruction.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ float4 make_img(double ux, double uy, double uz, int sp) {
   return make_float4((float)ux, (float)uy, (float)uz, __int_as_float(sp));
 }
@@ -192,7 +208,7 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
   float coef = 0.f;
   if (LJ) {
     if (r2 < k.rc2) {
-      const float ir2 = __frcp_rn(r2);
+      const float ir2 = rcp_approx(r2);
       const float sr2 = k.sig2 * ir2;
       const float sr6 = sr2 * sr2 * sr2;
       coef = -k.eps24 * ir2 * sr6 * (2.0f * sr6 - 1.0f);
@@ -209,9 +225,9 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
       if (REC) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
     }
   }
-  kahan_add(fx, cx, coef * dx);
-  kahan_add(fy, cy, coef * dy);
-  kahan_add(fz, cz, coef * dz);
+  kahan_fma(fx, cx, coef, dx);
+  kahan_fma(fy, cy, coef, dy);
+  kahan_fma(fz, cz, coef, dz);
 }
 
 // MODE 0: step (force, kick, record?, kick, drift, image, skin test); 1: last step of a block (force,
@@ -916,7 +932,11 @@ struct DescP {
 __global__ void __launch_bounds__(256) k_desc_engine(Eng E, int src, DescP P, const float* __restrict__ mean,
                                                       const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ X,
                                                       float* __restrict__ V) {
-  const int lane = threadIdx.x & 31;
+  // Two stages per chunk of 32 neighbours: (1) lanes split the neighbours and stage r, fc/r-weighted unit
+  // vector and species in shared memory; (2) each lane (one Gaussian channel) accumulates over the chunk.
+  __shared__ float4 stage[8][32];   // (dx/r, dy/r, dz/r, r) per neighbour
+  __shared__ float2 stage2[8][32];  // (fc, species)
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= E.S) return;
   const int r = E.tile_rep[i >> 5];
@@ -931,25 +951,48 @@ __global__ void __launch_bounds__(256) k_desc_engine(Eng E, int src, DescP P, co
     const float mu = P.r0 + lane * P.dmu;
     const int m = E.nnb[i];
     const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
-    for (int k = 0; k < m; ++k) {
-      const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
-      const float4 pj = im[e & kIdxMask];
-      const uint32_t code = e >> kIdxBits;
-      const float fx = (pj.x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
-      const float fy = (pj.y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
-      const float fz = (pj.z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
-      const float r2 = fx * fx + fy * fy + fz * fz;
-      if (!(r2 < P.rc2)) continue;
-      const float rr = sqrtf(r2);
-      const float fc = 0.5f * (__cosf(P.pi_rc * rr) + 1.0f);
-      const float t = rr - mu;
-      const float g = __expf(-t * t * P.inv2s2) * fc;
-      const float gr = g / rr;
-      const int s = __float_as_int(pj.w) & 1;
-      d[s] += g;
-      vx[s] += gr * fx;
-      vy[s] += gr * fy;
-      vz[s] += gr * fz;
+    for (int base = 0; base < m; base += 32) {
+      const int k = base + lane;
+      float4 st = make_float4(0.f, 0.f, 0.f, 1e30f);
+      float2 st2 = make_float2(0.f, 0.f);
+      bool inside = false;
+      if (k < m) {
+        const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
+        const float4 pj = im[e & kIdxMask];
+        const uint32_t code = e >> kIdxBits;
+        const float fx = (pj.x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
+        const float fy = (pj.y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
+        const float fz = (pj.z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
+        const float r2 = fx * fx + fy * fy + fz * fz;
+        if (r2 < P.rc2) {
+          const float rr = sqrtf(r2), ir = 1.0f / rr;
+          st = make_float4(fx * ir, fy * ir, fz * ir, rr);
+          st2 = make_float2(0.5f * (__cosf(P.pi_rc * rr) + 1.0f), (float)(__float_as_int(pj.w) & 1));
+          inside = true;
+        }
+      }
+      // keep only neighbours inside the descriptor cutoff, in list order
+      const unsigned bal = __ballot_sync(0xffffffffu, inside);
+      if (inside) {
+        const int pos = __popc(bal & ((1u << lane) - 1u));
+        stage[wib][pos] = st;
+        stage2[wib][pos] = st2;
+      }
+      __syncwarp();
+      const int cnt = __popc(bal);
+      for (int q = 0; q < cnt; ++q) {
+        const float4 a = stage[wib][q];
+        const float2 b = stage2[wib][q];
+        const float t = a.w - mu;
+        const float g = __expf(-t * t * P.inv2s2) * b.x;   // 0 for neighbours outside rc (fc = 0)
+        const int s = (int)b.y;
+        if (s == 0) {
+          d[0] += g; vx[0] += g * a.x; vy[0] += g * a.y; vz[0] += g * a.z;
+        } else {
+          d[1] += g; vx[1] += g * a.x; vy[1] += g * a.y; vz[1] += g * a.z;
+        }
+      }
+      __syncwarp();
     }
   }
   __nv_bfloat16* xrow = X + i * 80;
@@ -997,6 +1040,7 @@ struct acs_engine {
   float* c_V = nullptr;
   float* c_F = nullptr;
   int32_t* c_status = nullptr;
+  int c_stride = 1;          // refresh the correction every c_stride force evaluations (it is held in between)
   float last_corr_ms = 0.f;
 };
 
@@ -1249,7 +1293,7 @@ int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cud
     const int src = k & 1, dst = (k + 1) & 1;
     const bool last = (k == steps - 1);
     const int rec = rec_at[k] ? 1 : 0;
-    if ((st = launch_correction(e, src, s))) return st;
+    if (k % e->c_stride == 0 && (st = launch_correction(e, src, s))) return st;
     if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, s))) return st;
     if (!last || rec) {
       if ((st = launch_rebuild(e, dst, rec, rec_idx, 0, s))) return st;
@@ -1575,7 +1619,7 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
     const int src = k & 1, dst = (k + 1) & 1;
     const bool last = (k == steps - 1);
     const int rec = ((record_every > 0 && (k + 1) % record_every == 0) || last) ? 1 : 0;
-    if (e->corr) st = mark(2, [&] { return launch_correction(e, src, s); });
+    if (e->corr && k % e->c_stride == 0) st = mark(2, [&] { return launch_correction(e, src, s); });
     if (!st) st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, s); });
     if (!st) st = mark(1, [&] { return launch_rebuild(e, dst, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, 0, s); });
     rec_idx += rec;
@@ -1636,6 +1680,16 @@ int acs_engine_set_correction(acs_engine* e, const float* params6, const float* 
 }
 
 float acs_engine_last_correction_ms(acs_engine* e) { return e ? e->last_corr_ms : 0.f; }
+
+int acs_engine_set_correction_stride(acs_engine* e, int32_t stride) {
+  if (!e || stride < 1) return ACS_ERR_ARG;
+  if (stride != e->c_stride) {
+    for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    e->graphs.clear();
+  }
+  e->c_stride = stride;
+  return ACS_OK;
+}
 
 int acs_engine_destroy(acs_engine* e) {
   if (!e) return ACS_OK;

@@ -188,9 +188,27 @@ __device__ __forceinline__ void put(unsigned char* sm, uint32_t base, int r, int
   *reinterpret_cast<bf16*>(sm + base + umma::tile_offset(r, k, R)) = __float2bfloat16(v);
 }
 
-__device__ void load_tile(unsigned char* sm, uint32_t base, const bf16* __restrict__ src, int R, int K) {
-  for (int idx = threadIdx.x; idx < R * K; idx += blockDim.x)
-    *reinterpret_cast<bf16*>(sm + base + umma::tile_offset(idx / K, idx % K, R)) = src[idx];
+// Row-major [R x K] BF16 (global, 16-byte aligned rows) -> canonical tile: each 8-element row segment of a core
+// matrix is 16 contiguous bytes, moved with one vector load and store. Rows >= rows_valid are zero.
+__device__ void load_tile(unsigned char* sm, uint32_t base, const bf16* __restrict__ src, int R, int K,
+                          int rows_valid = 1 << 30) {
+  const int k8n = K / 8;
+  for (int c = threadIdx.x; c < R * k8n; c += blockDim.x) {
+    const int r = c / k8n, k8 = c % k8n;
+    const uint4 v = r < rows_valid ? *reinterpret_cast<const uint4*>(src + (int64_t)r * K + 8 * k8) : make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4*>(sm + base + umma::tile_offset(r, 8 * k8, R)) = v;
+  }
+}
+
+// One row of FP32 values (64) -> BF16 row r of a canonical tile, 16 bytes per store.
+__device__ __forceinline__ void put_row64(unsigned char* sm, uint32_t base, int r, int R, const float* v) {
+#pragma unroll
+  for (int k8 = 0; k8 < 8; ++k8) {
+    __nv_bfloat162 p[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) p[q] = __floats2bfloat162_rn(v[8 * k8 + 2 * q], v[8 * k8 + 2 * q + 1]);
+    *reinterpret_cast<uint4*>(sm + base + umma::tile_offset(r, 8 * k8, R)) = *reinterpret_cast<uint4*>(p);
+  }
 }
 
 // Issue D(+)= A[128 x K] B[N x K]^T (one elected thread), K in 16-wide slices.
@@ -260,11 +278,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
     load_tile(sm, MlpSmem::W2T, W.W2T, kH, kH);
     load_tile(sm, MlpSmem::W3T, W.W3T, kH, kOut);
   }
-  for (int idx = t; idx < kTile * kIn; idx += blockDim.x) {
-    const int r = idx / kIn, k = idx % kIn;
-    const bf16 v = (row0 + r < n) ? X[(row0 + r) * kIn + k] : __float2bfloat16(0.f);
-    *reinterpret_cast<bf16*>(sm + MlpSmem::X + umma::tile_offset(r, k, kTile)) = v;
-  }
+  load_tile(sm, MlpSmem::X, X + row0 * kIn, kTile, kIn, (int)min<int64_t>(kTile, n - row0));
   if (TRAIN) {  // weight-gradient A operand: rows 64..127 stay zero
     for (int idx = t; idx < kTile * kTile; idx += blockDim.x) put(sm, MlpSmem::GT, idx / kTile, idx % kTile, kTile, 0.f);
   }
@@ -279,11 +293,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   if (t == 0) gemm(sm, tm + kTZ1, MlpSmem::X, MlpSmem::W1, kH, kIn, kH);
   S.wait();
   read_row(tm, kTZ1, kH, z);
-  for (int q = 0; q < kH; ++q) {
-    const float h = silu(z[q]);
-    put(sm, MlpSmem::H1, t, q, kTile, h);
-    if (TRAIN) put(sm, MlpSmem::H1T, q, t, kGradCols, h);
-  }
+  for (int q = 0; q < kH; ++q) z[q] = silu(z[q]);
+  put_row64(sm, MlpSmem::H1, t, kTile, z);
+  if (TRAIN)
+    for (int q = 0; q < kH; ++q) put(sm, MlpSmem::H1T, q, t, kGradCols, z[q]);
   if (TRAIN) {
     put(sm, MlpSmem::H1T, 64, t, kGradCols, 1.f);
     for (int q = 65; q < kGradCols; ++q) put(sm, MlpSmem::H1T, q, t, kGradCols, 0.f);
@@ -293,11 +306,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   if (t == 0) gemm(sm, tm + kTZ2, MlpSmem::H1, MlpSmem::W2, kH, kH, kH);
   S.wait();
   read_row(tm, kTZ2, kH, z);
-  for (int q = 0; q < kH; ++q) {
-    const float h = silu(z[q] + W.b2[q]);
-    put(sm, MlpSmem::H2, t, q, kTile, h);
-    if (TRAIN) put(sm, MlpSmem::H2T, q, t, kGradCols, h);
-  }
+  for (int q = 0; q < kH; ++q) z[q] = silu(z[q] + W.b2[q]);
+  put_row64(sm, MlpSmem::H2, t, kTile, z);
+  if (TRAIN)
+    for (int q = 0; q < kH; ++q) put(sm, MlpSmem::H2T, q, t, kGradCols, z[q]);
   if (TRAIN) {
     put(sm, MlpSmem::H2T, 64, t, kGradCols, 1.f);
     for (int q = 65; q < kGradCols; ++q) put(sm, MlpSmem::H2T, q, t, kGradCols, 0.f);

@@ -72,6 +72,7 @@ ENGINE_SIGNATURES = {
     "acs_engine_phase_times": (C.c_int, [P, P, C.c_int]),
     "acs_engine_set_correction": (C.c_int, [P, P, P, P, P, P, P, C.c_float, P, P, P, P, C.c_int]),
     "acs_engine_last_correction_ms": (C.c_float, [P]),
+    "acs_engine_set_correction_stride": (C.c_int, [P, C.c_int32]),
     "acs_engine_destroy": (C.c_int, [P]),
 }
 _lib.SIGNATURES.update(ENGINE_SIGNATURES)
@@ -230,6 +231,9 @@ class Engine:
                                                     self._cF.data_ptr(), m.status.ptr, 1), "acs_engine_set_correction")
         self.correction = lc
 
+    def set_correction_stride(self, stride):
+        _lib.check(self.L.acs_engine_set_correction_stride(self.h, int(stride)), "acs_engine_set_correction_stride")
+
     def last_correction_ms(self):
         return float(self.L.acs_engine_last_correction_ms(self.h))
 
@@ -362,7 +366,7 @@ class GpuSimulation:
     `run` call (and at records when positions=True)."""
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
-                 rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500):
+                 rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500, correction_stride=1):
         from .integrators import VelocityVerlet
         from .simulation import Trajectory
         from .units import si
@@ -387,6 +391,7 @@ class GpuSimulation:
         self.correction = None
         self.validate_every = int(validate_every)
         self.validations = []
+        self.engine.set_correction_stride(correction_stride)
         if correction is not None:
             self.set_correction(correction)
         self._last = self.engine.records(1)[0, 0]

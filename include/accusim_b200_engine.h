@@ -93,6 +93,9 @@ int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear);
 int acs_engine_set_correction(acs_engine* e, const float* params6, const float* mean, const float* inv_std,
                               const void* const* w5, const float* b2, const float* b3, float out_scale, void* X,
                               float* V, float* F, int32_t* status_dev, int enabled);
+/* Refresh the correction every `stride` force evaluations of a block (the first of each block always) and
+ * hold it in between (a multiple-time-step treatment of this slowly varying force). Default 1. */
+int acs_engine_set_correction_stride(acs_engine* e, int32_t stride);
 /* Mean duration (ms) of the correction launches in the last acs_engine_run_timed call. */
 float acs_engine_last_correction_ms(acs_engine* e);
 int acs_engine_destroy(acs_engine* e);
