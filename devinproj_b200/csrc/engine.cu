@@ -929,13 +929,22 @@ struct DescP {
   float r0, dmu, inv2s2, rc2, pi_rc;
 };
 
-__global__ void __launch_bounds__(256) k_desc_engine(Eng E, int src, DescP P, const float* __restrict__ mean,
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__global__ void __launch_bounds__(256, 4) k_desc_engine(Eng E, int src, DescP P, const float* __restrict__ mean,
                                                       const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ X,
                                                       float* __restrict__ V) {
-  // Two stages per chunk of 32 neighbours: (1) lanes split the neighbours and stage r, fc/r-weighted unit
-  // vector and species in shared memory; (2) each lane (one Gaussian channel) accumulates over the chunk.
-  __shared__ float4 stage[8][32];   // (dx/r, dy/r, dz/r, r) per neighbour
-  __shared__ float2 stage2[8][32];  // (fc, species)
+  // Per pass, 4 chunks of 32 neighbours: (1) lanes split the neighbours (list entries, then positions, each
+  // batch of loads in flight together) and stage r, the unit vector, fc and species of those inside the
+  // descriptor cutoff in shared memory, in list order; (2) each lane (one Gaussian channel) accumulates over
+  // the staged neighbours.
+  constexpr int kU = 4;
+  __shared__ float4 stage[8][32 * kU];   // (dx/r, dy/r, dz/r, r) per neighbour
+  __shared__ float stage2[8][32 * kU];   // log2(fc)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= E.S) return;
@@ -951,46 +960,58 @@ __global__ void __launch_bounds__(256) k_desc_engine(Eng E, int src, DescP P, co
     const float mu = P.r0 + lane * P.dmu;
     const int m = E.nnb[i];
     const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
-    for (int base = 0; base < m; base += 32) {
-      const int k = base + lane;
-      float4 st = make_float4(0.f, 0.f, 0.f, 1e30f);
-      float2 st2 = make_float2(0.f, 0.f);
-      bool inside = false;
-      if (k < m) {
-        const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
-        const float4 pj = im[e & kIdxMask];
-        const uint32_t code = e >> kIdxBits;
-        const float fx = (pj.x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
-        const float fy = (pj.y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
-        const float fz = (pj.z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
-        const float r2 = fx * fx + fy * fy + fz * fz;
-        if (r2 < P.rc2) {
-          const float rr = sqrtf(r2), ir = 1.0f / rr;
-          st = make_float4(fx * ir, fy * ir, fz * ir, rr);
-          st2 = make_float2(0.5f * (__cosf(P.pi_rc * rr) + 1.0f), (float)(__float_as_int(pj.w) & 1));
-          inside = true;
-        }
+    for (int base = 0; base < m; base += 32 * kU) {
+      uint32_t e[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = base + 32 * u + lane;
+        e[u] = k < m ? (uint32_t)lst[(int64_t)k * E.G] : 0u;
       }
-      // keep only neighbours inside the descriptor cutoff, in list order
-      const unsigned bal = __ballot_sync(0xffffffffu, inside);
-      if (inside) {
-        const int pos = __popc(bal & ((1u << lane) - 1u));
-        stage[wib][pos] = st;
-        stage2[wib][pos] = st2;
+      float4 pj[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = base + 32 * u + lane;
+        pj[u] = k < m ? im[e[u] & kIdxMask] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      // species 0 staged from the front, species 1 from the back, each in list order
+      int cnt0 = 0, cnt1 = 0;
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = base + 32 * u + lane;
+        const uint32_t code = e[u] >> kIdxBits;
+        const float fx = (pj[u].x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
+        const float fy = (pj[u].y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
+        const float fz = (pj[u].z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
+        const float r2 = fx * fx + fy * fy + fz * fz;
+        const bool inside = k < m && r2 < P.rc2;
+        const bool s1 = (__float_as_int(pj[u].w) & 1) != 0;
+        const unsigned b0 = __ballot_sync(0xffffffffu, inside && !s1), b1 = __ballot_sync(0xffffffffu, inside && s1);
+        if (inside) {
+          const float ir = rsqrtf(r2), rr = r2 * ir;
+          const unsigned lt = (1u << lane) - 1u;
+          const int pos = s1 ? (32 * kU - 1) - (cnt1 + __popc(b1 & lt)) : cnt0 + __popc(b0 & lt);
+          stage[wib][pos] = make_float4(fx * ir, fy * ir, fz * ir, rr);
+          // the cosine cutoff enters the exponent: g fc = 2^(-(r - mu)^2 k log2(e) + log2(fc))
+          stage2[wib][pos] = __log2f(0.5f * (__cosf(P.pi_rc * rr) + 1.0f));
+        }
+        cnt0 += __popc(b0);
+        cnt1 += __popc(b1);
       }
       __syncwarp();
-      const int cnt = __popc(bal);
-      for (int q = 0; q < cnt; ++q) {
+      const float k2 = P.inv2s2 * 1.4426950408889634f;
+#pragma unroll 4
+      for (int q = 0; q < cnt0; ++q) {
         const float4 a = stage[wib][q];
-        const float2 b = stage2[wib][q];
         const float t = a.w - mu;
-        const float g = __expf(-t * t * P.inv2s2) * b.x;   // 0 for neighbours outside rc (fc = 0)
-        const int s = (int)b.y;
-        if (s == 0) {
-          d[0] += g; vx[0] += g * a.x; vy[0] += g * a.y; vz[0] += g * a.z;
-        } else {
-          d[1] += g; vx[1] += g * a.x; vy[1] += g * a.y; vz[1] += g * a.z;
-        }
+        const float g = ex2_approx(fmaf(-t * t, k2, stage2[wib][q]));
+        d[0] += g; vx[0] = fmaf(g, a.x, vx[0]); vy[0] = fmaf(g, a.y, vy[0]); vz[0] = fmaf(g, a.z, vz[0]);
+      }
+#pragma unroll 4
+      for (int q = 32 * kU - cnt1; q < 32 * kU; ++q) {
+        const float4 a = stage[wib][q];
+        const float t = a.w - mu;
+        const float g = ex2_approx(fmaf(-t * t, k2, stage2[wib][q]));
+        d[1] += g; vx[1] = fmaf(g, a.x, vx[1]); vy[1] = fmaf(g, a.y, vy[1]); vz[1] = fmaf(g, a.z, vz[1]);
       }
       __syncwarp();
     }

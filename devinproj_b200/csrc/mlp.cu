@@ -175,12 +175,28 @@ struct MlpSmem {  // byte offsets into dynamic shared memory
 };
 static_assert(MlpSmem::END <= 227 * 1024, "MLP shared-memory plan exceeds 227 KB");
 
+// Inference needs neither the transposed weights nor the gradient buffers; it stages the tile's vector
+// features instead: row r (64 x 3 FP32 = 768 B) at VS + r * kVRow. The 16-byte pad makes the per-row
+// 16-byte reads of 8 consecutive threads cover all 32 banks.
+constexpr uint32_t kVRowBytes = kOut * 3 * 4, kVRow = kVRowBytes + 16;
+struct MlpSmemInf {
+  static constexpr uint32_t H1 = MlpSmem::W3 + kOut * kH * 2;   // 128 x 64
+  static constexpr uint32_t H2 = H1 + kTile * kH * 2;          // 128 x 64
+  static constexpr uint32_t VS = H2 + kTile * kH * 2;          // 128 rows of kVRow bytes
+  static constexpr uint32_t B = VS + kTile * kVRow;            // b2, b3 (FP32, 128)
+  static constexpr uint32_t FP = B + 2 * 64 * 4;               // second-half partial forces (128 x 3 FP32)
+  static constexpr uint32_t END = FP + kTile * 3 * 4;
+};
+static_assert(MlpSmemInf::END <= 227 * 1024 && MlpSmemInf::VS % 16 == 0, "MLP inference shared-memory plan");
+
 // TMEM columns: Z1 [0,64), Z2 [64,128), C [128,192), activation-gradient D [192,256), weight-gradient D [256,336)
 constexpr uint32_t kTZ1 = 0, kTZ2 = 64, kTC = 128, kTdH = 192, kTdW = 256, kTCols = 512;
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// Approximate division (MUFU reciprocal): the results are rounded to BF16 next, far coarser than its error.
+// For z -> -inf, 1 + e^-z -> inf and both return 0.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -189,15 +205,23 @@ __device__ __forceinline__ void put(unsigned char* sm, uint32_t base, int r, int
 }
 
 // Row-major [R x K] BF16 (global, 16-byte aligned rows) -> canonical tile: each 8-element row segment of a core
-// matrix is 16 contiguous bytes, moved with one vector load and store. Rows >= rows_valid are zero.
-__device__ void load_tile(unsigned char* sm, uint32_t base, const bf16* __restrict__ src, int R, int K,
-                          int rows_valid = 1 << 30) {
+// matrix is 16 contiguous bytes, moved with one asynchronous 16-byte copy (all of a thread's copies are in
+// flight together; cp_async_wait() completes them). Rows >= rows_valid are zero-filled.
+__device__ __forceinline__ void load_tile(unsigned char* sm, uint32_t base, const bf16* __restrict__ src, int R, int K,
+                                          int rows_valid = 1 << 30) {
   const int k8n = K / 8;
   for (int c = threadIdx.x; c < R * k8n; c += blockDim.x) {
     const int r = c / k8n, k8 = c % k8n;
-    const uint4 v = r < rows_valid ? *reinterpret_cast<const uint4*>(src + (int64_t)r * K + 8 * k8) : make_uint4(0, 0, 0, 0);
-    *reinterpret_cast<uint4*>(sm + base + umma::tile_offset(r, 8 * k8, R)) = v;
+    const uint32_t dst = umma::smem_u32(sm + base + umma::tile_offset(r, 8 * k8, R));
+    const bool in = r < rows_valid;
+    const bf16* g = in ? src + (int64_t)r * K + 8 * k8 : src;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(g), "r"(in ? 16 : 0) : "memory");
   }
+}
+
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // One row of FP32 values (64) -> BF16 row r of a canonical tile, 16 bytes per store.
@@ -265,10 +289,14 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
+  constexpr uint32_t kH1 = MlpSmem::H1, kH2 = MlpSmem::H2;
   const int t = threadIdx.x, warp = t >> 5;
   const int64_t row0 = (int64_t)blockIdx.x * kTile;
   const int64_t gi = row0 + t;
   const bool valid = gi < n;
+  const int rows = (int)(n - row0 < kTile ? n - row0 : kTile);
+
+  if (t == 0) umma::mbar_init(&mbar, 1);
 
   // operands: weights and this tile's inputs (rows past n are zero)
   load_tile(sm, MlpSmem::W1, W.W1, kH, kIn);
@@ -278,12 +306,12 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
     load_tile(sm, MlpSmem::W2T, W.W2T, kH, kH);
     load_tile(sm, MlpSmem::W3T, W.W3T, kH, kOut);
   }
-  load_tile(sm, MlpSmem::X, X + row0 * kIn, kTile, kIn, (int)min<int64_t>(kTile, n - row0));
+  load_tile(sm, MlpSmem::X, X + row0 * kIn, kTile, kIn, rows);
   if (TRAIN) {  // weight-gradient A operand: rows 64..127 stay zero
     for (int idx = t; idx < kTile * kTile; idx += blockDim.x) put(sm, MlpSmem::GT, idx / kTile, idx % kTile, kTile, 0.f);
   }
-  if (t == 0) umma::mbar_init(&mbar, 1);
   if (warp == 0) umma::tmem_alloc(&tslot, kTCols);
+  cp_async_wait();
   smem_to_mma();
   const uint32_t tm = tslot;
   Sync S{&mbar, 0u, status, true};
@@ -294,7 +322,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   S.wait();
   read_row(tm, kTZ1, kH, z);
   for (int q = 0; q < kH; ++q) z[q] = silu(z[q]);
-  put_row64(sm, MlpSmem::H1, t, kTile, z);
+  put_row64(sm, kH1, t, kTile, z);
   if (TRAIN)
     for (int q = 0; q < kH; ++q) put(sm, MlpSmem::H1T, q, t, kGradCols, z[q]);
   if (TRAIN) {
@@ -303,11 +331,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   }
   smem_to_mma();
   // ---- layer 2
-  if (t == 0) gemm(sm, tm + kTZ2, MlpSmem::H1, MlpSmem::W2, kH, kH, kH);
+  if (t == 0) gemm(sm, tm + kTZ2, kH1, MlpSmem::W2, kH, kH, kH);
   S.wait();
   read_row(tm, kTZ2, kH, z);
   for (int q = 0; q < kH; ++q) z[q] = silu(z[q] + W.b2[q]);
-  put_row64(sm, MlpSmem::H2, t, kTile, z);
+  put_row64(sm, kH2, t, kTile, z);
   if (TRAIN)
     for (int q = 0; q < kH; ++q) put(sm, MlpSmem::H2T, q, t, kGradCols, z[q]);
   if (TRAIN) {
@@ -316,7 +344,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   }
   smem_to_mma();
   // ---- layer 3: coefficients, contraction with the vector features
-  if (t == 0) gemm(sm, tm + kTC, MlpSmem::H2, MlpSmem::W3, kOut, kH, kOut);
+  if (t == 0) gemm(sm, tm + kTC, kH2, MlpSmem::W3, kOut, kH, kOut);
   S.wait();
   read_row(tm, kTC, kOut, c);
   float F[3] = {0.f, 0.f, 0.f};
@@ -413,6 +441,127 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const bf16* __restrict__ X, cons
   if (warp == 0) umma::tmem_free(tm, kTCols);
 }
 
+// Inference on one 128-ion tile with 256 threads. Warps w and w + 4 share TMEM lane quadrant w % 4 (rows
+// 32 (w % 4) + lane) and split every epilogue's columns: half h = w / 4 takes [32 h, 32 h + 32). The tile's
+// vector features stream into shared memory (bulk copies) behind the three layers; the two halves of the
+// contraction F = sum_c C_c V_c meet in shared memory.
+constexpr uint32_t kInfCols = 256;  // TMEM: Z1 [0, 64), Z2 [64, 128), C [128, 192)
+
+__device__ __forceinline__ void read32(uint32_t tmem, int quad, uint32_t col, float* out) {
+  float v[16];
+  umma::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + col, v);
+#pragma unroll
+  for (int q = 0; q < 16; ++q) out[q] = v[q];
+  umma::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + col + 16u, v);
+#pragma unroll
+  for (int q = 0; q < 16; ++q) out[16 + q] = v[q];
+}
+
+// 32 FP32 values -> BF16 columns [8 k8_0, 8 k8_0 + 32) of row r of a canonical tile, 16 bytes per store.
+__device__ __forceinline__ void put_row32(unsigned char* sm, uint32_t base, int r, int R, int k8_0, const float* v) {
+#pragma unroll
+  for (int k8 = 0; k8 < 4; ++k8) {
+    __nv_bfloat162 p[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) p[q] = __floats2bfloat162_rn(v[8 * k8 + 2 * q], v[8 * k8 + 2 * q + 1]);
+    *reinterpret_cast<uint4*>(sm + base + umma::tile_offset(r, 8 * (k8_0 + k8), R)) = *reinterpret_cast<uint4*>(p);
+  }
+}
+
+__global__ void __launch_bounds__(256, 1) k_mlp_infer(const bf16* __restrict__ X, const float* __restrict__ V, int64_t n,
+                                                      MlpWeights W, float out_scale, float* __restrict__ Fout,
+                                                      int* status) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ uint64_t mbar, vbar;
+  __shared__ uint32_t tslot;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int quad = warp & 3, half = warp >> 2;
+  const int row = 32 * quad + lane;
+  const int64_t row0 = (int64_t)blockIdx.x * kTile;
+  const int64_t gi = row0 + row;
+  const bool valid = gi < n;
+  const int rows = (int)(n - row0 < kTile ? n - row0 : kTile);
+  float* bias = reinterpret_cast<float*>(sm + MlpSmemInf::B);
+  float* fpart = reinterpret_cast<float*>(sm + MlpSmemInf::FP);
+
+  if (t == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::mbar_init(&vbar, 1);
+    umma::mbar_fence_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane == 0) umma::mbar_expect_tx(&vbar, (uint32_t)rows * kVRowBytes);
+    __syncwarp();
+    for (int r = lane; r < rows; r += 32)
+      umma::bulk_g2s(umma::smem_u32(sm + MlpSmemInf::VS + r * kVRow), V + (row0 + r) * kOut * 3, kVRowBytes, &vbar);
+  }
+  load_tile(sm, MlpSmem::W1, W.W1, kH, kIn);
+  load_tile(sm, MlpSmem::W2, W.W2, kH, kH);
+  load_tile(sm, MlpSmem::W3, W.W3, kOut, kH);
+  load_tile(sm, MlpSmem::X, X + row0 * kIn, kTile, kIn, rows);
+  if (t < 128) bias[t] = t < 64 ? W.b2[t] : W.b3[t - 64];
+  if (warp == 0) umma::tmem_alloc(&tslot, kInfCols);
+  cp_async_wait();
+  smem_to_mma();
+  const uint32_t tm = tslot;
+  Sync S{&mbar, 0u, status, true};
+  const uint32_t col = 32u * (uint32_t)half;
+  float z[32];
+
+  if (t == 0) gemm(sm, tm + kTZ1, MlpSmem::X, MlpSmem::W1, kH, kIn, kH);
+  S.wait();
+  read32(tm, quad, kTZ1 + col, z);
+#pragma unroll
+  for (int q = 0; q < 32; ++q) z[q] = silu(z[q]);
+  put_row32(sm, MlpSmemInf::H1, row, kTile, 4 * half, z);
+  smem_to_mma();
+
+  if (t == 0) gemm(sm, tm + kTZ2, MlpSmemInf::H1, MlpSmem::W2, kH, kH, kH);
+  S.wait();
+  read32(tm, quad, kTZ2 + col, z);
+#pragma unroll
+  for (int q = 0; q < 32; ++q) z[q] = silu(z[q] + bias[col + q]);
+  put_row32(sm, MlpSmemInf::H2, row, kTile, 4 * half, z);
+  smem_to_mma();
+
+  if (t == 0) gemm(sm, tm + kTC, MlpSmemInf::H2, MlpSmem::W3, kOut, kH, kOut);
+  S.wait();
+  read32(tm, quad, kTC + col, z);
+  bool have_v = umma::mbar_wait(&vbar, 0);
+  if (!have_v) {
+    if (t == 0) atomicOr(status, ACS_FLAG_TIMEOUT);
+    umma::mbar_wait(&vbar, 0);  // second bounded wait for copies still in flight
+  }
+  // this half's channels q in [32 h, 32 h + 32) are the row's FP32 elements [96 h, 96 h + 96)
+  float F[3] = {0.f, 0.f, 0.f};
+  if (valid && have_v) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) z[q] += bias[64 + col + q];
+    const float4* vr = reinterpret_cast<const float4*>(sm + MlpSmemInf::VS + row * kVRow) + 24 * half;
+#pragma unroll
+    for (int m = 0; m < 24; ++m) {
+      const float4 v = vr[m];
+      const float e4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) F[(4 * m + j) % 3] = fmaf(z[(4 * m + j) / 3], e4[j], F[(4 * m + j) % 3]);
+    }
+  }
+  if (half == 1) {
+    fpart[3 * row] = F[0];
+    fpart[3 * row + 1] = F[1];
+    fpart[3 * row + 2] = F[2];
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (half == 0 && valid && have_v) {
+    Fout[3 * gi] = out_scale * (F[0] + fpart[3 * row]);
+    Fout[3 * gi + 1] = out_scale * (F[1] + fpart[3 * row + 1]);
+    Fout[3 * gi + 2] = out_scale * (F[2] + fpart[3 * row + 2]);
+  }
+  if (warp == 0) umma::tmem_free(tm, kInfCols);
+}
+
 // Sum the per-tile gradient partials in tile order (deterministic) and take an Adam step on the FP32
 // master parameters; refresh the BF16 operand copies (W and the transposes of W2, W3).
 // Parameter vector: [W1 64x80 | W2aug 64x80 (cols 0..63 weights, 64 bias) | W3aug 64x80], FP32.
@@ -489,19 +638,20 @@ int32_t acs_mlp_param_count(void) { return 3 * kH * kGradCols; }
 int acs_mlp_forward(const void* X, const float* V, int64_t n, const void* const* w5, const float* b2, const float* b3,
                     float out_scale, float* F, int32_t* status_dev, void* stream) {
   if (n < 1 || !X || !V || !w5 || !b2 || !b3 || !F || !status_dev) return ACS_ERR_ARG;
-  const size_t smem = MlpSmem::END;
+  if ((uintptr_t)V & 15) return ACS_ERR_ARG;   // rows are bulk-copied: 16-byte alignment
+  const size_t smem = MlpSmemInf::END;
   // set once per device: this launch may sit inside a CUDA graph capture
   static bool attr_set[64] = {false};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ACS_ERR_NO_DEVICE;
   if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return ACS_ERR_CUDA;
     attr_set[dev] = true;
   }
   MlpWeights W{(const bf16*)w5[0], (const bf16*)w5[1], (const bf16*)w5[2], (const bf16*)w5[3], (const bf16*)w5[4], b2, b3};
-  k_mlp<false><<<(int)ceil_div(n, kTile), 128, smem, (cudaStream_t)stream>>>((const bf16*)X, V, nullptr, n, W, out_scale,
-                                                                            0.f, F, nullptr, nullptr, status_dev);
+  k_mlp_infer<<<(int)ceil_div(n, kTile), 256, smem, (cudaStream_t)stream>>>((const bf16*)X, V, n, W, out_scale, F,
+                                                                             status_dev);
   return launch_status();
 }
 

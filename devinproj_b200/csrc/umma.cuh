@@ -59,6 +59,21 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, int count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count));
 }
 
+// Makes mbarrier initialisation visible to the async proxy (bulk copies complete on the barrier).
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Arrive on the barrier and add `bytes` to the transaction count the current phase waits for.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// Bulk copy (no tensor map, no multicast) global -> this CTA's shared memory, completing `bytes` on the
+// barrier. Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(mbar)) : "memory");
+}
+
 // Bounded wait for the mbarrier phase; false after `limit` polls (the caller reports a timeout).
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t phase, long long limit = 4000000) {
   const uint32_t a = smem_u32(mbar);

@@ -127,6 +127,27 @@ def test_descriptors_match_fp64_oracle():
     assert np.all(X[:, 79] == 1.0) and np.all(X[np.arange(s.n), 64 + s.sp] == 1.0)
 
 
+def test_engine_descriptors_match_fp64_oracle():
+    """The descriptors the engine computes inside its step (FP32 images, shift-coded neighbour list) against
+    the FP64 oracle on the same state; same tolerances as the stand-alone kernel."""
+    from devinproj_b200 import GpuSimulation, configs
+    from devinproj_b200.engine import LEN
+    from devinproj_b200.learned import LearnedCorrection
+    from oracle import mlp_port
+    s, forces = configs.nacl_melt(8, rcut=10e-10, seed=3)
+    s.pos = (s.pos + np.random.default_rng(1).normal(0, 0.3e-10, s.pos.shape)) % s.box
+    lc = LearnedCorrection(seed=0)
+    sim = GpuSimulation(s, forces, dt=1e-15, correction=lc, validate_every=0)
+    X = sim.engine._cX[: s.n].float().cpu().numpy()
+    V = sim.engine._cV[: s.n].cpu().numpy()
+    p = lc.desc.p
+    D_ref, V_ref = mlp_port.descriptors(s.pos / LEN, s.sp, s.box / LEN, p["rc"], p["r0"], p["dmu"], p["s"])
+    assert np.max(np.abs(V - V_ref)) <= 1e-4 * np.max(np.abs(V_ref))
+    X_ref = mlp_port.inputs(D_ref, s.sp, np.zeros(64), np.ones(64))
+    assert np.max(np.abs(X - X_ref)) <= 1e-2 * np.max(np.abs(X_ref))
+    assert np.all(X[:, 79] == 1.0) and np.all(X[np.arange(s.n), 64 + s.sp] == 1.0)
+
+
 def test_learned_correction_beats_plain_dsf_on_held_out_melt():
     """Small-scale version of the learned DSF->Ewald correction: 512-ion melt, labels from the device Ewald
     (pinned to the reference above); the corrected forces must be closer to Ewald than plain DSF on
