@@ -447,6 +447,14 @@ def run_experiment(args):
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
         e0, e1 = lc.errors(d, np.arange(n_train, args.snapshots))
+        # floor of any pair-additive correction of range R (least squares on the same labels)
+        from devinproj_b200.learned import pair_kernel_bound
+        fit_idx = np.arange(min(n_train, 100))
+        test_idx = np.arange(n_train, min(args.snapshots, n_train + 20))
+        bound = {}
+        for R in (10.0, 15.0, 20.0):
+            b0, b1 = pair_kernel_bound(d, fit_idx, test_idx, R * 1e-10)
+            bound[f"{R:g}A"] = {"err_dsf": b0, "err_fit": b1, "ratio": b0 / b1}
         # step-time overhead of the correction on the 8000-ion melt (eager per-kernel timing)
         s, forces, dt = configs.nacl8000()
         s.pos = d["pos"][-1].copy()
@@ -459,30 +467,32 @@ def run_experiment(args):
         c_ms = corr.engine.last_correction_ms()
         step_plain = t_plain / 200
         step_corr = step_plain + c_ms
-        stride = 10
-        corr.engine.set_correction_stride(stride)
-        corr.engine.run(20, 0, True)
-        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e_a.record()
-        corr.engine.run(200, 0, True)
-        e_b.record()
-        plain_a, plain_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        plain.engine.run(200, 0, True)
-        torch.cuda.synchronize()
-        plain_a.record()
-        plain.engine.run(200, 0, True)
-        plain_b.record()
-        torch.cuda.synchronize()
-        graph_corr = e_a.elapsed_time(e_b) / 200
-        graph_plain = plain_a.elapsed_time(plain_b) / 200
+        def graph_ms(engine, steps=200):
+            engine.run(steps, 0, True)   # same block length as the timed run: its graph is captured here
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            engine.run(steps, 0, True)
+            b.record()
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / steps
+
+        graph_plain = graph_ms(plain.engine)
+        graph_corr = {}
+        for stride in (1, 5, 10, 25):
+            corr.engine.set_correction_stride(stride)
+            graph_corr[stride] = graph_ms(corr.engine)
         print(json.dumps({"experiment": "learned_dsf_correction", "ions": 8000, "snapshots": args.snapshots,
                           "train_snapshots": n_train, "dataset_s": t_gen, "train_s": t_train,
                           "train_loss_first_last": [hist[0], hist[-1]],
                           "heldout_rms_rel_err_dsf": e0, "heldout_rms_rel_err_corrected": e1, "error_ratio": e0 / e1,
+                          "pair_kernel_bound": bound,
                           "step_ms_plain": step_plain, "correction_ms": c_ms,
                           "overhead_frac": c_ms / step_plain, "step_ms_corrected": step_corr,
-                          "graph_ms_per_step_plain": graph_plain, "graph_ms_per_step_corrected_stride10": graph_corr,
-                          "overhead_frac_stride10": graph_corr / graph_plain - 1.0}), flush=True)
+                          "graph_ms_per_step_plain": graph_plain,
+                          "graph_ms_per_step_corrected": {f"stride{k}": v for k, v in graph_corr.items()},
+                          "graph_overhead_frac": {f"stride{k}": v / graph_plain - 1.0 for k, v in graph_corr.items()}}),
+              flush=True)
     elif args.experiment == "drift":
         from devinproj_b200.engine import start_engine
         s, forces, dt, cfg = workload("lj1m", seed=0)

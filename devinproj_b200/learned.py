@@ -228,6 +228,61 @@ def generate_dataset(n_snapshots, seed=0, n_sites=20, T=1300.0, melt_T=4000.0, m
                 species=[(x.name, x.mass, x.charge) for x in s.species], T=T)
 
 
+def pair_kernel_bound(data, train_idx, test_idx, R, spacing=0.25e-10, device="cuda", chunk=512):
+    """How far any correction built from pair terms within R can go: fit the residual F_Ewald - F_DSF as
+    sum_{j: r_ij < R} q_i q_j h_t(r_ij) r_hat_ij, with one free radial function h_t per species pair
+    (piecewise linear on a `spacing` grid), by least squares over the train snapshots. Every pair-additive
+    electrostatic correction of range R, DSF's own kernel included, is one such function, so the fitted
+    error is a floor for them; the learned network sees the same 10 A neighbourhood through its descriptors.
+    Returns (mean RMS relative error of plain DSF, of the fitted correction) against Ewald on test
+    snapshots. Analysis only (torch FP64), not part of the step path."""
+    f64 = torch.float64
+    box = torch.as_tensor(np.asarray(data["box"], float), dtype=f64, device=device)
+    sp = torch.as_tensor(np.asarray(data["sp"]), dtype=torch.long, device=device)
+    qs = np.array([c for (_, _, c) in data["species"]], float)
+    q = torch.as_tensor(qs / np.max(np.abs(qs)), dtype=f64, device=device)[sp]
+    nb = int(math.ceil(R / spacing)) + 1
+    nf = 3 * nb
+
+    def feats(k):
+        pos = torch.as_tensor(data["pos"][k], dtype=f64, device=device)
+        n = pos.shape[0]
+        phi = torch.zeros((n, nf, 3), dtype=f64, device=device)
+        for i0 in range(0, n, chunk):
+            d = pos[None, :, :] - pos[i0:i0 + chunk, None, :]
+            d -= box * torch.round(d / box)
+            r = torch.linalg.norm(d, dim=-1)
+            ii, jj = torch.nonzero((r < R) & (r > 0), as_tuple=True)
+            rr = r[ii, jj]
+            vec = (q[i0 + ii] * q[jj] / rr)[:, None] * d[ii, jj]
+            x = rr / spacing
+            b0 = torch.floor(x)
+            w1 = (x - b0)[:, None]
+            col = (sp[i0 + ii] + sp[jj]) * nb + b0.long()
+            rows = i0 + ii
+            phi.index_put_((rows, col), (1.0 - w1) * vec, accumulate=True)
+            phi.index_put_((rows, col + 1), w1 * vec, accumulate=True)
+        return phi
+
+    G = torch.zeros((nf, nf), dtype=f64, device=device)
+    h = torch.zeros(nf, dtype=f64, device=device)
+    for k in train_idx:
+        phi = feats(k)
+        y = torch.as_tensor(data["residual"][k], dtype=f64, device=device)
+        A = phi.permute(0, 2, 1).reshape(-1, nf)
+        G += A.T @ A
+        h += A.T @ y.reshape(-1)
+    ridge = 1e-9 * torch.trace(G) / nf
+    w = torch.linalg.solve(G + ridge * torch.eye(nf, dtype=f64, device=device), h)
+    e0, e1 = [], []
+    for k in test_idx:
+        pred = torch.einsum("nfc,f->nc", feats(k), w).cpu().numpy()
+        Fe = data["dsf"][k] + data["residual"][k]
+        e0.append(rms_rel(data["dsf"][k], Fe))
+        e1.append(rms_rel(data["dsf"][k] + pred, Fe))
+    return float(np.mean(e0)), float(np.mean(e1))
+
+
 class LearnedCorrection:
     """DSF + learned residual: fit on a dataset, predict corrections, judge against Ewald."""
 
