@@ -548,6 +548,20 @@ struct PairScan {
   }
 };
 
+// Exact decision for a candidate in the FP32 band around the list radius, on a replica with >= 3 cells per
+// axis: the reference's FP64 filter on the absolute positions (minimum image by comparison with box/2).
+// Kept out of line so the candidate loop branches around it instead of issuing it predicated.
+__device__ __noinline__ bool band_accept(const double* __restrict__ xa, int64_t i, int64_t k, double L0, double L1,
+                                         double L2, double rl2) {
+  double dx = sub(xa[3 * k], xa[3 * i]);
+  double dy = sub(xa[3 * k + 1], xa[3 * i + 1]);
+  double dz = sub(xa[3 * k + 2], xa[3 * i + 2]);
+  if (dx > 0.5 * L0) dx = sub(dx, L0); else if (dx < -0.5 * L0) dx = sub(dx, -L0);
+  if (dy > 0.5 * L1) dy = sub(dy, L1); else if (dy < -0.5 * L1) dy = sub(dy, -L1);
+  if (dz > 0.5 * L2) dz = sub(dz, L2); else if (dz < -0.5 * L2) dz = sub(dz, -L2);
+  return norm2(dx, dy, dz) < rl2;
+}
+
 // Rebuild of flagged replicas and per-replica record reduction. Cooperative launch (all blocks resident);
 // every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging.
 __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
@@ -788,11 +802,131 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       if (lane == 0) ps.finish(cnt);
     }
   } else {
+    // Replicas with >= 3 cells on every axis: a warp per home cell. The candidates of the 27 stencil cells, in
+    // list order (stencil cell, then ascending slot), are packed 32 to a batch, one per lane, with the cell
+    // pair's image shift already added. For each home atom h (up to 32, staged in shared memory) the warp
+    // tests all 32 candidates at once; two ballots give home atom h its masks (accepted / inside the upper
+    // band edge), which lane h keeps. The next batch is loaded while this one is screened; only the FP64
+    // band decision branches.
+    __shared__ float4 hpos[8][32];
+    __shared__ uint32_t candk[8][32];
+    const int64_t gw = gtid >> 5, nw = gstride >> 5;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int64_t c = gw; c < E.C; c += nw) {
+      const int r = E.cell_rep[c];
+      if (!fl[r]) continue;
+      const RepDev& R = E.rep[r];
+      if (R.nc[0] < 3 || R.nc[1] < 3 || R.nc[2] < 3 || c - R.cellbase >= R.ncells) continue;
+      const float4* __restrict__ im = E.img[dst];
+      const float rl2f = (float)R.rl2, lo_f = rl2f * (1.0f - 1e-4f), hi_f = rl2f * (1.0f + 1e-4f);
+      // stencil cell st = 9 (a + 1) + 3 (b + 1) + (d + 1) in list order: lane st holds its first slot, its
+      // length and the exclusive prefix P of the lengths (its first position in the packed sequence)
+      int sk0 = 0, slen = 0;
+      if (lane < 27) {
+        int c0, c1, c2;
+        cell_coords((int)(c - R.cellbase), R, c0, c1, c2);
+        const int n0 = wrapc(c0 + lane / 9 - 1, R.nc[0]), n1 = wrapc(c1 + (lane / 3) % 3 - 1, R.nc[1]),
+                  n2 = wrapc(c2 + lane % 3 - 1, R.nc[2]);
+        const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + n2;
+        sk0 = E.start[cc];
+        slen = E.start[cc + 1] - sk0;
+      }
+      int incl = slen;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int P = incl - slen;
+      const int T = __shfl_sync(0xffffffffu, incl, 26);
+      const int h0 = __shfl_sync(0xffffffffu, sk0, 13), hn = __shfl_sync(0xffffffffu, slen, 13);
+      const int P13 = __shfl_sync(0xffffffffu, P, 13);
+      // this lane's candidate at packed position pb + lane: shifted position and list entry (slot | code)
+      auto stage = [&](int pb, float4& cp, uint32_t& ck) {
+        const int p = pb + lane;
+        const int pp = p < T ? p : T - 1;
+        int st = 0;   // last stencil cell with P <= pp
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int cs = st + step;
+          const int Pc = __shfl_sync(0xffffffffu, P, cs < 27 ? cs : 26);
+          if (cs < 27 && Pc <= pp) st = cs;
+        }
+        const int k = __shfl_sync(0xffffffffu, sk0, st) + (pp - __shfl_sync(0xffffffffu, P, st));
+        cp = make_float4(3e30f, 3e30f, 3e30f, 0.f);   // padding: r^2 overflows, never accepted
+        ck = 0u;
+        if (p < T) {
+          const int a = st / 9 - 1, b = (st / 3) % 3 - 1, d = st % 3 - 1;
+          const float4 pj = im[k];
+          cp = make_float4(pj.x + a * R.csf[0], pj.y + b * R.csf[1], pj.z + d * R.csf[2], 0.f);
+          ck = (uint32_t)k | ((uint32_t)((a + 1) + 3 * (b + 1) + 9 * (d + 1)) << kIdxBits);
+        }
+      };
+      for (int hb = 0; hb < hn; hb += 32) {
+        const int nh = min(32, hn - hb);
+        const bool own = lane < nh;
+        const int64_t i = h0 + hb + (own ? lane : 0);
+        __syncwarp();
+        hpos[wib][lane] = im[i];
+        int32_t* __restrict__ lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
+        int cnt = 0;
+        float4 cp;
+        uint32_t ck;
+        stage(0, cp, ck);
+        for (int pb = 0; pb < T; pb += 32) {
+          __syncwarp();
+          candk[wib][lane] = ck;
+          const float4 cur = cp;
+          __syncwarp();
+          if (pb + 32 < T) stage(pb + 32, cp, ck);   // in flight while this batch is screened
+          uint32_t m_in = 0u, m_hi = 0u;
+#pragma unroll 2
+          for (int h = 0; h < nh; ++h) {
+            const float4 hp = hpos[wib][h];
+            const float x = cur.x - hp.x, y = cur.y - hp.y, z = cur.z - hp.z;
+            const float q = x * x + y * y + z * z;
+            const unsigned bi = __ballot_sync(0xffffffffu, q <= lo_f), bh = __ballot_sync(0xffffffffu, q < hi_f);
+            if (lane == h) {
+              m_in = bi;
+              m_hi = bh;
+            }
+          }
+          const int self = P13 + hb + lane - pb;   // packed position of atom i in this batch
+          if (self >= 0 && self < 32) {
+            m_in &= ~(1u << self);
+            m_hi &= ~(1u << self);
+          }
+          if (!own) m_in = m_hi = 0u;
+          uint32_t m_band = m_hi & ~m_in;
+          if (__any_sync(0xffffffffu, m_band != 0u)) {
+            while (m_band) {
+              const int t = __ffs(m_band) - 1;
+              m_band &= m_band - 1u;
+              if (band_accept(E.tmp_xa, i, candk[wib][t] & kIdxMask, R.L[0], R.L[1], R.L[2], R.rl2)) m_in |= 1u << t;
+            }
+          }
+          while (m_in) {   // list order
+            const int t = __ffs(m_in) - 1;
+            m_in &= m_in - 1u;
+            if (cnt < E.maxnb) lst[(int64_t)cnt * E.G] = (int32_t)candk[wib][t];
+            ++cnt;
+          }
+        }
+        if (own) {
+          E.nnb[i] = min(cnt, E.maxnb);
+          if (cnt > E.maxnb) {
+            atomicOr(&E.status->flags, ACS_FLAG_OVERFLOW);
+            atomicMax(&E.status->need_nbr, cnt);
+          }
+        }
+      }
+    }
+    // Replicas with a one-cell axis (small boxes): a thread per atom with the per-axis wrap.
     for (int64_t i = gtid; i < E.S; i += gstride) {
       const int r = E.tile_rep[i >> 5];
       if (!fl[r]) continue;
       const RepDev& R = E.rep[r];
-      if (i - R.atom0 >= R.n) continue;
+      if (i - R.atom0 >= R.n || !(R.nc[0] < 3 || R.nc[1] < 3 || R.nc[2] < 3)) continue;
       PairScan ps(E, R, i, dst);
       int cnt = 0;
       for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
