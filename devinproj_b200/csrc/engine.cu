@@ -194,8 +194,9 @@ __device__ __forceinline__ PairK pair_consts(const FFDev& ff, int p, const PairK
   return k;
 }
 
-// One pair: accumulate f_i += coef * d (Kahan) and, when recording, the pair energy (Kahan).
-template <bool LJ, bool DSF, bool REC, bool ONE>
+// One pair: accumulate f_i += coef * d (Kahan; with KAHAN false a plain FP32 block partial that the caller
+// adds to the Kahan sums) and, when recording, the pair energy (Kahan).
+template <bool LJ, bool DSF, bool REC, bool ONE, bool KAHAN = true>
 __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int sio, const float4& pi, uint32_t e,
                                           const float4& pj, const float4* shift_row, float& fx, float& fy, float& fz,
                                           float& cx, float& cy, float& cz, float& eu, float& ce) {
@@ -206,14 +207,13 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
   const float r2 = dx * dx + dy * dy + dz * dz;
   const PairK k = pair_consts<ONE>(ff, ONE ? 0 : sio + __float_as_int(pj.w), c1);
   float coef = 0.f;
-  if (LJ) {
-    if (r2 < k.rc2) {
-      const float ir2 = rcp_approx(r2);
-      const float sr2 = k.sig2 * ir2;
-      const float sr6 = sr2 * sr2 * sr2;
-      coef = -k.eps24 * ir2 * sr6 * (2.0f * sr6 - 1.0f);
-      if (REC) kahan_add(eu, ce, k.eps4 * (sr6 * sr6 - sr6) - k.ushift);
-    }
+  if (LJ) {  // evaluated for every entry and selected: no divergent branch in the pair loop
+    const float ir2 = rcp_approx(r2);
+    const float sr2 = k.sig2 * ir2;
+    const float sr6 = sr2 * sr2 * sr2;
+    const bool in = r2 < k.rc2;
+    coef = in ? -k.eps24 * ir2 * sr6 * (2.0f * sr6 - 1.0f) : 0.f;
+    if (REC && in) kahan_add(eu, ce, k.eps4 * (sr6 * sr6 - sr6) - k.ushift);
   }
   if (DSF) {
     if (r2 < ff.dsf_rc2) {
@@ -225,9 +225,15 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
       if (REC) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
     }
   }
-  kahan_fma(fx, cx, coef, dx);
-  kahan_fma(fy, cy, coef, dy);
-  kahan_fma(fz, cz, coef, dz);
+  if (KAHAN) {
+    kahan_fma(fx, cx, coef, dx);
+    kahan_fma(fy, cy, coef, dy);
+    kahan_fma(fz, cz, coef, dz);
+  } else {
+    fx = fmaf(coef, dx, fx);
+    fy = fmaf(coef, dy, fy);
+    fz = fmaf(coef, dz, fz);
+  }
 }
 
 // MODE 0: step (force, kick, record?, kick, drift, image, skin test); 1: last step of a block (force,
@@ -298,9 +304,14 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
 #pragma unroll
           for (int q = 0; q < 4; ++q) en[q] = (uint32_t)__ldcs(lst + (t + 4 + q) * 32);
         }
+        // the four pair forces are summed in FP32, the block sum enters the Kahan sums
+        float bx = 0.f, by = 0.f, bz = 0.f, bcx, bcy, bcz;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e[q], pj[q], shift_row, fx, fy, fz, cx, cy, cz, eu, ce);
+          pair_term<LJ, DSF, REC, ONE, false>(ff, c1, sio, pi, e[q], pj[q], shift_row, bx, by, bz, bcx, bcy, bcz, eu, ce);
+        kahan_add(fx, cx, bx);
+        kahan_add(fy, cy, by);
+        kahan_add(fz, cz, bz);
       }
       for (; t < n_it; ++t) {
         const uint32_t e = (uint32_t)__ldcs(lst + t * 32);
@@ -408,14 +419,6 @@ __global__ void k_prologue(Eng E, int dst) {
   }
 }
 
-__device__ __forceinline__ void stencil(int c, int nc, int& lo, int& hi) {
-  if (nc >= 3) {
-    lo = -1;
-    hi = 1;
-  } else {
-    lo = 0;
-    hi = 0;
-  }
 }
 
 __device__ __forceinline__ int wrapc(int c, int nc) { return c < 0 ? c + nc : (c >= nc ? c - nc : c); }
