@@ -419,8 +419,6 @@ __global__ void k_prologue(Eng E, int dst) {
   }
 }
 
-}
-
 __device__ __forceinline__ int wrapc(int c, int nc) { return c < 0 ? c + nc : (c >= nc ? c - nc : c); }
 
 __device__ int block_scan_excl(int v, int* total) {
