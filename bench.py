@@ -198,7 +198,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
-    ap.add_argument("--experiment", choices=["learned", "drift", "dropin"], default=None,
+    ap.add_argument("--experiment", choices=["learned", "drift", "dropin", "correction_kernels"], default=None,
                     help="accuracy experiments (one JSON line each): the learned DSF->Ewald correction at full scale, "
                          "the 1e4-step energy drift of the 1M-atom run, the plain FP64 drop-in's throughput")
     ap.add_argument("--snapshots", type=int, default=2000)
@@ -493,6 +493,17 @@ def run_experiment(args):
                           "graph_ms_per_step_corrected": {f"stride{k}": v for k, v in graph_corr.items()},
                           "graph_overhead_frac": {f"stride{k}": v / graph_plain - 1.0 for k, v in graph_corr.items()}}),
               flush=True)
+    elif args.experiment == "correction_kernels":
+        # the correction's kernels inside the step loop on the 8000-ion melt (untrained weights: the kernels'
+        # work does not depend on the weights); eager launches with per-kernel events
+        from devinproj_b200 import GpuSimulation, configs
+        from devinproj_b200.learned import LearnedCorrection
+        s, forces, dt = configs.nacl8000()
+        sim = GpuSimulation(s, forces, dt=dt, correction=LearnedCorrection(seed=0), validate_every=0)
+        step_ms, list_ms, _ = sim.engine.run_timed(max(args.steps, 1), 0)
+        print(json.dumps({"experiment": "correction_kernels", "ions": s.n, "steps": args.steps,
+                          "step_kernel_ms": step_ms, "list_kernel_ms": list_ms,
+                          "correction_ms": sim.engine.last_correction_ms()}), flush=True)
     elif args.experiment == "drift":
         from devinproj_b200.engine import start_engine
         s, forces, dt, cfg = workload("lj1m", seed=0)
