@@ -8,12 +8,12 @@ from .engine import GpuSimulation
 from .ewald import Ewald
 from .learned import LearnedCorrection
 from .forces import DampedShiftedCoulomb, Force, LennardJones, VerletList, cell_list_pairs
-from .integrators import Integrator, VelocityVerlet
+from .integrators import Integrator, Langevin, NoseHoover, VelocityVerlet
 from .simulation import Simulation, Trajectory
 from .system import Species, System
 from .units import k_B, k_e
 
 __all__ = ["AccuracyReport", "Ewald", "GpuSimulation", "LearnedCorrection", "DampedShiftedCoulomb", "Force", "Integrator", "LennardJones", "Simulation",
-           "Species", "System", "Trajectory", "VelocityVerlet", "VerletList", "calibrate_dt", "cell_list_pairs",
+           "Langevin", "NoseHoover", "Species", "System", "Trajectory", "VelocityVerlet", "VerletList", "calibrate_dt", "cell_list_pairs",
            "k_B", "k_e", "timestep_convergence"]
 __version__ = "0.1.0"

@@ -46,6 +46,7 @@ SIGNATURES = {
     "acs_lj_fp64_noalloc": (C.c_int, [P, P, I64, P, C.c_int, P, P, I32, I32, P, P, DBL, P, P, P]),
     "acs_dsf_fp64": (C.c_int, [P, P, I64, P, C.c_int, P, P, I32, P, P, DBL, DBL, DBL, P, P, P, SZ, P]),
     "acs_vv_kick": (C.c_int, [P, P, I64, DBL, P]),
+    "acs_langevin_ou": (C.c_int, [P, P, P, I64, DBL, P]),
     "acs_vv_drift_wrap": (C.c_int, [P, P, I64, DBL, P, C.c_int, P]),
     "acs_vv_accel": (C.c_int, [P, P, P, P, I32, I64, P]),
     "acs_reduce_work_bytes": (SZ, [I64]),

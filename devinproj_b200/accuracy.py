@@ -8,6 +8,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from .units import k_B
+
 from .units import si
 
 PASS, WARN, FAIL, NA = "PASS", "WARN", "FAIL", "n/a"
@@ -85,6 +87,14 @@ class AccuracyReport:
                                 "max |E(t)-E0| / energy scale (incl. reaction ledger)"))
         else:
             checks.append(Check("energy", NA, None, "not conserved by design"))
+        if hasattr(integ, "bath_energy") and all(f.conservative for f in sim.forces) and len(tr.bath) == len(tr.t):
+            # accusim/accuracy.py:81-84: the Nose-Hoover conserved quantity
+            E = tr.total_energy
+            scale = max(abs(E[0]), np.max(np.abs(tr.kinetic)), np.max(np.abs(tr.potential)), 1e-300)
+            Ex = E + np.array(tr.bath)
+            dx = float(np.max(np.abs(Ex - Ex[0])) / scale)
+            checks.append(Check("extended energy", _grade(dx, 1e-5, 1e-3), dx,
+                                "Nose-Hoover conserved quantity: E + thermostat energy"))
         if not external and not walls and not integ.thermostat:
             dp = momentum_drift(tr, s)
             checks.append(Check("momentum", _grade(dp, 1e-9, 1e-6), dp, "max |P(t)-P0| / sum m|v|"))
@@ -105,6 +115,18 @@ class AccuracyReport:
         qscale = max(float(np.sum(np.abs(s.charges))), 1e-300)
         dq = float(np.max(np.abs(Qc - Qc[0])) / qscale)
         checks.append(Check("charge", _grade(dq, 1e-12, 1e-9), dq, "total charge"))
+        kind = type(integ).__name__
+        if kind in ("Langevin", "NoseHoover") and len(tr.t) >= 4:
+            # accusim/accuracy.py:112-123: mean temperature over the second half against the target
+            half = len(tr.t) // 2
+            kin = np.asarray(tr.kinetic[half:])
+            n = np.array([sum(c.values()) for c in tr.counts[half:]], dtype=float)
+            dof = s.dim * np.maximum(n - 1, 1) if kind == "NoseHoover" else s.dim * np.maximum(n, 1)
+            T_meas = float(np.mean(2 * kin / (dof * k_B)))
+            dev = abs(T_meas - integ.T) / integ.T
+            tol = max(0.02, 3 * np.sqrt(2 / (s.dim * max(s.n, 1))))
+            checks.append(Check("thermostat", PASS if dev <= tol else (WARN if dev <= 0.1 else FAIL), dev,
+                                f"mean T over 2nd half {T_meas:.4g} K vs target {integ.T:.4g} K"))
         if convergence_duration is not None:
             checks.append(timestep_convergence(sim, convergence_duration))
         return cls(checks)

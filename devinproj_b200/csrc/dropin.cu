@@ -355,6 +355,13 @@ __global__ void k_drift_wrap(double* __restrict__ pos, const double* __restrict_
   }
 }
 
+// Langevin O-step: vel = c1 * vel + sig[atom] * noise (accusim/integrators.py:66-67, no FMA).
+__global__ void k_langevin_ou(double* __restrict__ vel, const double* __restrict__ noise,
+                              const double* __restrict__ sig, int64_t n3, double c1) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) vel[i] = add(mul(c1, vel[i]), mul(sig[i / 3], noise[i]));
+}
+
 struct MassTab {
   double m[ACS_MAX_SPECIES];
 };
@@ -622,6 +629,13 @@ int acs_vv_drift_wrap(double* pos, const double* vel, int64_t n, double dt, cons
   if (n == 0) return ACS_OK;
   k_drift_wrap<<<(int)ceil_div(n, kBlock), kBlock, 0, (cudaStream_t)stream>>>(pos, vel, n, dt,
                                                                                 make_box(box3, periodic));
+  return launch_status();
+}
+
+int acs_langevin_ou(double* vel, const double* noise, const double* sig, int64_t n, double c1, void* stream) {
+  if (n < 0 || (n > 0 && (!vel || !noise || !sig))) return ACS_ERR_ARG;
+  if (n == 0) return ACS_OK;
+  k_langevin_ou<<<(int)ceil_div(3 * n, kBlock), kBlock, 0, (cudaStream_t)stream>>>(vel, noise, sig, 3 * n, c1);
   return launch_status();
 }
 

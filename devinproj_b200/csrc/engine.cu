@@ -804,15 +804,20 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     }
   } else {
     // Replicas with >= 3 cells on every axis: a warp per home cell. The candidates of the 27 stencil cells, in
-    // list order (stencil cell, then ascending slot), are packed 32 to a batch, one per lane, with the cell
-    // pair's image shift already added. For each home atom h (up to 32, staged in shared memory) the warp
-    // tests all 32 candidates at once; two ballots give home atom h its masks (accepted / inside the upper
-    // band edge), which lane h keeps. The next batch is loaded while this one is screened; only the FP64
-    // band decision branches.
+    // list order (stencil cell, then ascending slot), are read 32 at a time with the cell pair's image shift
+    // already added; those whose distance to the home cell's box exceeds the list radius (with the band
+    // margin) cannot pair with any home atom and are dropped, the rest are compacted in order into a
+    // shared-memory buffer. Each full batch of 32 is screened against the home atoms (up to 32, staged in
+    // shared memory): for home atom h, two ballots over the batch give its masks (accepted / inside the
+    // upper band edge), which lane h keeps. The next raw chunk is loaded while a batch is screened; only the
+    // FP64 band decision branches.
     __shared__ float4 hpos[8][32];
-    __shared__ uint32_t candk[8][32];
+    __shared__ float4 bufp[8][64];
+    __shared__ uint32_t bufk[8][64];
+    __shared__ int selfpos[8][32];
     const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     for (int64_t c = gw; c < E.C; c += nw) {
       const int r = E.cell_rep[c];
       if (!fl[r]) continue;
@@ -841,9 +846,9 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       const int P = incl - slen;
       const int T = __shfl_sync(0xffffffffu, incl, 26);
       const int h0 = __shfl_sync(0xffffffffu, sk0, 13), hn = __shfl_sync(0xffffffffu, slen, 13);
-      const int P13 = __shfl_sync(0xffffffffu, P, 13);
-      // this lane's candidate at packed position pb + lane: shifted position and list entry (slot | code)
-      auto stage = [&](int pb, float4& cp, uint32_t& ck) {
+      // this lane's raw candidate at packed position pb + lane: shifted position, list entry (slot | code)
+      // and whether it can reach the home cell's box [0, cs)^3 within the list radius
+      auto stage = [&](int pb, float4& cp, uint32_t& ck, bool& keep) {
         const int p = pb + lane;
         const int pp = p < T ? p : T - 1;
         int st = 0;   // last stencil cell with P <= pp
@@ -854,32 +859,59 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           if (cs < 27 && Pc <= pp) st = cs;
         }
         const int k = __shfl_sync(0xffffffffu, sk0, st) + (pp - __shfl_sync(0xffffffffu, P, st));
-        cp = make_float4(3e30f, 3e30f, 3e30f, 0.f);   // padding: r^2 overflows, never accepted
+        keep = false;
         ck = 0u;
+        cp = make_float4(0.f, 0.f, 0.f, 0.f);
         if (p < T) {
           const int a = st / 9 - 1, b = (st / 3) % 3 - 1, d = st % 3 - 1;
           const float4 pj = im[k];
           cp = make_float4(pj.x + a * R.csf[0], pj.y + b * R.csf[1], pj.z + d * R.csf[2], 0.f);
           ck = (uint32_t)k | ((uint32_t)((a + 1) + 3 * (b + 1) + 9 * (d + 1)) << kIdxBits);
+          const float gx = fmaxf(fmaxf(-cp.x, cp.x - R.csf[0]), 0.f);
+          const float gy = fmaxf(fmaxf(-cp.y, cp.y - R.csf[1]), 0.f);
+          const float gz = fmaxf(fmaxf(-cp.z, cp.z - R.csf[2]), 0.f);
+          keep = gx * gx + gy * gy + gz * gz < hi_f;
         }
       };
       for (int hb = 0; hb < hn; hb += 32) {
         const int nh = min(32, hn - hb);
         const bool own = lane < nh;
         const int64_t i = h0 + hb + (own ? lane : 0);
+        const uint32_t hlo = (uint32_t)(h0 + hb);
         __syncwarp();
         hpos[wib][lane] = im[i];
         int32_t* __restrict__ lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
-        int cnt = 0;
-        float4 cp;
-        uint32_t ck;
-        stage(0, cp, ck);
-        for (int pb = 0; pb < T; pb += 32) {
+        int cnt = 0, nbuf = 0, rb = 0;
+        float4 rp;
+        uint32_t rk;
+        bool rkeep;
+        stage(0, rp, rk, rkeep);
+        while (true) {
+          if (rb < T) {   // append this raw chunk's survivors, in order
+            const unsigned bal = __ballot_sync(0xffffffffu, rkeep);
+            if (rkeep) {
+              const int pos = nbuf + __popc(bal & lt_mask);
+              bufp[wib][pos] = rp;
+              bufk[wib][pos] = rk;
+            }
+            nbuf += __popc(bal);
+            rb += 32;
+            if (rb < T) stage(rb, rp, rk, rkeep);   // in flight while a batch is screened
+          }
+          if (nbuf == 0 && rb >= T) break;
+          if (nbuf < 32 && rb < T) continue;
+          const int nk = min(32, nbuf);
           __syncwarp();
-          candk[wib][lane] = ck;
-          const float4 cur = cp;
+          float4 cur = make_float4(3e30f, 3e30f, 3e30f, 0.f);   // padding: r^2 overflows, never accepted
+          uint32_t ck = 0u;
+          if (lane < nk) {
+            cur = bufp[wib][lane];
+            ck = bufk[wib][lane];
+          }
+          selfpos[wib][lane] = -1;
           __syncwarp();
-          if (pb + 32 < T) stage(pb + 32, cp, ck);   // in flight while this batch is screened
+          const uint32_t hs = (ck & kIdxMask) - hlo;   // home index of this candidate, if it is a home atom
+          if (lane < nk && hs < (uint32_t)nh) selfpos[wib][hs] = lane;
           uint32_t m_in = 0u, m_hi = 0u;
 #pragma unroll 2
           for (int h = 0; h < nh; ++h) {
@@ -892,8 +924,9 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
               m_hi = bh;
             }
           }
-          const int self = P13 + hb + lane - pb;   // packed position of atom i in this batch
-          if (self >= 0 && self < 32) {
+          __syncwarp();
+          const int self = selfpos[wib][lane];   // never the atom itself
+          if (self >= 0) {
             m_in &= ~(1u << self);
             m_hi &= ~(1u << self);
           }
@@ -903,15 +936,30 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
             while (m_band) {
               const int t = __ffs(m_band) - 1;
               m_band &= m_band - 1u;
-              if (band_accept(E.tmp_xa, i, candk[wib][t] & kIdxMask, R.L[0], R.L[1], R.L[2], R.rl2)) m_in |= 1u << t;
+              if (band_accept(E.tmp_xa, i, bufk[wib][t] & kIdxMask, R.L[0], R.L[1], R.L[2], R.rl2)) m_in |= 1u << t;
             }
           }
           while (m_in) {   // list order
             const int t = __ffs(m_in) - 1;
             m_in &= m_in - 1u;
-            if (cnt < E.maxnb) lst[(int64_t)cnt * E.G] = (int32_t)candk[wib][t];
+            if (cnt < E.maxnb) lst[(int64_t)cnt * E.G] = (int32_t)bufk[wib][t];
             ++cnt;
           }
+          // keep the survivors beyond this batch at the front of the buffer
+          __syncwarp();
+          const int rest = nbuf - nk;
+          float4 mp = make_float4(0.f, 0.f, 0.f, 0.f);
+          uint32_t mk = 0u;
+          if (lane < rest) {
+            mp = bufp[wib][nk + lane];
+            mk = bufk[wib][nk + lane];
+          }
+          __syncwarp();
+          if (lane < rest) {
+            bufp[wib][lane] = mp;
+            bufk[wib][lane] = mk;
+          }
+          nbuf = rest;
         }
         if (own) {
           E.nnb[i] = min(cnt, E.maxnb);

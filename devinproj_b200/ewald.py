@@ -75,7 +75,8 @@ class Ewald(Force):
         F = torch.empty((n, 3), dtype=torch.float64, device="cuda")
         e3 = torch.zeros(3, dtype=torch.float64, device="cuda")
         ws = self._ws.get(L.acs_ewald_work_bytes(n, K))
-        _lib.check(L.acs_ewald_fp64(pos_d.data_ptr(), to_dev(q.astype(np.float64)).data_ptr(), n, box.ctypes.data,
+        q_d = to_dev(q.astype(np.float64))   # held until the launch: a freed tensor's memory is handed out again
+        _lib.check(L.acs_ewald_fp64(pos_d.data_ptr(), q_d.data_ptr(), n, box.ctypes.data,
                                     kv.data_ptr(), w.data_ptr(), K, float(a), float(rcut), float(self.k), F.data_ptr(),
                                     e3.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()), "acs_ewald_fp64")
         e = e3.cpu().numpy()

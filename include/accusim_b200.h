@@ -14,6 +14,7 @@
  *   acs_dsf_fp64                 accusim/forces.py:408-452 DampedShiftedCoulomb.compute
  *   acs_vv_*                     accusim/integrators.py:25-31 VelocityVerlet.step,
  *                                accusim/system.py:124-129 apply_boundaries, simulation.py:67-70
+ *   acs_langevin_ou              accusim/integrators.py:50-71 Langevin.step (the O-step; B and A reuse acs_vv_*)
  *   acs_reduce_conserved         accusim/system.py:106-114 kinetic_energy / momentum / angular_momentum
  *   acs_engine_*                 accusim/simulation.py:95-112 Simulation.run driving VelocityVerlet with
  *                                LennardJones and/or DampedShiftedCoulomb (device-resident fast path)
@@ -125,6 +126,10 @@ int acs_dsf_fp64(const double* pos, const double* q, int64_t n, const double* bo
 int acs_vv_kick(double* vel, const double* acc, int64_t n, double half_dt, void* stream);
 int acs_vv_drift_wrap(double* pos, const double* vel, int64_t n, double dt, const double* box3, int periodic,
                       void* stream);
+/* Langevin BAOAB O-step, replaces accusim/integrators.py:65-67 (Langevin.step): vel = c1 * vel + sig[i] *
+ * noise with c1 = exp(-gamma dt) and sig[i] = sqrt((1 - c1^2) kT / m_i) computed by the caller, noise the
+ * caller's standard normal draws (n x 3). The half drifts around it are acs_vv_drift_wrap with dt / 2. */
+int acs_langevin_ou(double* vel, const double* noise, const double* sig, int64_t n, double c1, void* stream);
 /* acc = force / mass[species] (accusim/simulation.py:70). */
 int acs_vv_accel(double* acc, const double* force, const int32_t* sp, const double* species_mass, int32_t n_species,
                  int64_t n, void* stream);

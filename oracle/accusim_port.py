@@ -395,14 +395,76 @@ def angular_momentum(st):      # accusim/system.py:112-114
     return np.atleast_1d(np.sum(L, axis=0))
 
 
-class Run:
-    """Simulation.run with VelocityVerlet and per-step records: accusim/simulation.py:95-112,
-    accusim/integrators.py:25-31, record fields of accusim/simulation.py:76-93."""
+class LangevinBAOAB:
+    """BAOAB Langevin step: accusim/integrators.py:50-71. `normal(shape)` supplies the standard normal
+    draws (the reference uses `sim.rng.normal`)."""
 
-    def __init__(self, st, forces, dt):
+    def __init__(self, T, gamma, normal):
+        self.T, self.gamma, self.normal = float(T), float(gamma), normal
+
+    def step(self, run, dt):
+        st = run.st
+        st.vel += 0.5 * dt * run.acc
+        st.pos += 0.5 * dt * st.vel
+        c1 = np.exp(-self.gamma * dt)
+        sig = np.sqrt((1 - c1 ** 2) * K_B * self.T / st.masses)[:, None]
+        st.vel = c1 * st.vel + sig * self.normal(st.vel.shape)
+        st.pos += 0.5 * dt * st.vel
+        apply_boundaries(st)
+        run.update_forces()
+        st.vel += 0.5 * dt * run.acc
+
+
+class NoseHooverMTK:
+    """Nose-Hoover with the Trotter half-steps of accusim/integrators.py:74-116 (thermostat mass
+    Q = N_f kT tau^2, N_f = dim (n - 1)); bath energy Q xi^2 / 2 + N_f kT eta."""
+
+    def __init__(self, T, tau):
+        self.T, self.tau = float(T), float(tau)
+        self.xi, self.eta, self.Q = 0.0, 0.0, None
+
+    @staticmethod
+    def dof(st):
+        return st.dim * max(st.n - 1, 1)
+
+    def half(self, st, dt):
+        kT, nf = K_B * self.T, self.dof(st)
+        if self.Q is None:
+            self.Q = nf * kT * self.tau ** 2
+        k2 = float(np.sum(st.masses[:, None] * st.vel ** 2))
+        self.xi += 0.25 * dt * (k2 - nf * kT) / self.Q
+        scale = np.exp(-0.5 * dt * self.xi)
+        st.vel *= scale
+        self.eta += 0.5 * dt * self.xi
+        self.xi += 0.25 * dt * (k2 * scale ** 2 - nf * kT) / self.Q
+
+    def step(self, run, dt):
+        st = run.st
+        self.half(st, dt)
+        st.vel += 0.5 * dt * run.acc
+        st.pos += dt * st.vel
+        apply_boundaries(st)
+        run.update_forces()
+        st.vel += 0.5 * dt * run.acc
+        self.half(st, dt)
+
+    def bath_energy(self, st):
+        if self.Q is None:
+            return 0.0
+        return 0.5 * self.Q * self.xi ** 2 + self.dof(st) * K_B * self.T * self.eta
+
+
+class Run:
+    """Simulation.run with per-step records: accusim/simulation.py:95-112, record fields of
+    accusim/simulation.py:76-93. The integrator is VelocityVerlet (accusim/integrators.py:25-31) unless an
+    object with `step(run, dt)` (LangevinBAOAB, NoseHooverMTK) is given."""
+
+    def __init__(self, st, forces, dt, integrator=None):
         self.st, self.forces, self.dt = st, forces, float(dt)
+        self.integrator = integrator
         self.time = 0.0
         self.t, self.kinetic, self.potential, self.momentum, self.angular_momentum = [], [], [], [], []
+        self.bath = []
         self.update_forces()
 
     def update_forces(self):
@@ -418,9 +480,14 @@ class Run:
         self.potential.append(self.pe)
         self.momentum.append(momentum(st))
         self.angular_momentum.append(angular_momentum(st))
+        bath = getattr(self.integrator, "bath_energy", None)
+        self.bath.append(bath(st) if bath else 0.0)
 
     def step(self):
         """accusim/integrators.py:25-31."""
+        if self.integrator is not None:
+            self.integrator.step(self, self.dt)
+            return
         st, dt = self.st, self.dt
         st.vel += 0.5 * dt * self.acc
         st.pos += dt * st.vel

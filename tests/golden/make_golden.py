@@ -13,6 +13,7 @@ Each case restates a reference test or example setup (file:line inside the accus
   dsf_skin                tests/test_dsf.py:119-139     Verlet skin == fresh list, rebuild count
   nacl4096                examples/molten_salt.py:22-33 geometry at the 4096-ion / 1.55 g/cm^3 config
   ewald_melt512           tests/test_dsf.py:46-52       Ewald label oracle on a disordered melt
+  thermostats108          tests/test_nose_hoover.py:6-17 argon; Langevin BAOAB and Nose-Hoover runs
 """
 from __future__ import annotations
 
@@ -26,6 +27,7 @@ REF = os.environ.get("ACCUSIM_REF", "/root/reference")
 sys.path.insert(0, REF)
 import accusim  # noqa: E402
 from accusim import Q, Simulation, System, VelocityVerlet, k_B  # noqa: E402
+from accusim.integrators import Langevin, NoseHoover  # noqa: E402
 from accusim.forces import DampedShiftedCoulomb, Ewald, LennardJones, cell_list_pairs  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -205,6 +207,32 @@ def ewald_melt():
     save("ewald_melt512", **state_arrays(s), F=Fe, U=Ue, F_dsf=Fd, U_dsf=Ud, dsf_rcut=3.9, dsf_alpha=0.6)
 
 
+def thermostats108():
+    """108 argon atoms (fcc 3^3 at 1374 kg/m^3, 60 K) under Langevin (120 K, 5e12 1/s, seed 11) and
+    Nose-Hoover (120 K, 0.2 ps), 40 steps of 5 fs each, records every 10 steps."""
+    m = Q(39.948, "u").value
+    L = (4 * 27 * m / 1374.0) ** (1 / 3)
+    out = {}
+    for name in ("lv", "nh"):
+        s = System(3, box=L, periodic=True)
+        s.add_species("Ar", m)
+        s.add("Ar", fcc(3, L))
+        s.maxwell_boltzmann(60.0, np.random.default_rng(3))
+        if name == "lv":
+            out.update({k + "0": v for k, v in state_arrays(s).items()})
+        lj = LennardJones({"Ar": (120 * k_B.value, 3.4e-10)}, cutoff=2.5)
+        integ = Langevin(120.0, 5e12) if name == "lv" else NoseHoover(120.0, Q(0.2, "ps"))
+        sim = Simulation(s, [lj], integrator=integ, dt=Q(5, "fs"), seed=11)
+        tr = sim.run(steps=40, record_every=10, positions=False)
+        out.update({f"{name}_pos": s.pos.copy(), f"{name}_vel": s.vel.copy(), f"{name}_acc": sim.acc.copy(),
+                    f"{name}_kinetic": np.array(tr.kinetic), f"{name}_potential": np.array(tr.potential),
+                    f"{name}_bath": np.array(tr.bath)})
+        if name == "nh":
+            out.update(nh_xi=integ.xi, nh_eta=integ.eta, nh_Q=integ.Q)
+    save("thermostats108", **out, eps=120 * k_B.value, sig=3.4e-10, dt=Q(5, "fs").value, steps=40, record_every=10,
+         T=120.0, friction=5e12, seed=11, tau=Q(0.2, "ps").value)
+
+
 if __name__ == "__main__":
     print("reference accusim", accusim.__version__, "from", os.path.dirname(accusim.__file__))
     lj_mix(True)
@@ -214,3 +242,4 @@ if __name__ == "__main__":
     dsf_cases()
     nacl4096()
     ewald_melt()
+    thermostats108()

@@ -289,3 +289,51 @@ def test_list_capacity_overflow_regrows():
     oi, oj = port.cell_list_pairs(st, 1.0)
     assert np.array_equal(pair_keys(i, j, s.n), pair_keys(oi, oj, s.n))
     assert nl.maxnb >= int(nl.nnb.max().item())
+
+
+@pytest.mark.parametrize("kind", ["lv", "nh"])
+def test_dropin_thermostats_match_reference(golden, kind):
+    """The Langevin (BAOAB, normal draws from `sim.rng` as the reference takes them) and Nose-Hoover
+    plug-ins inside `Simulation.run`: 40 steps of 108 argon atoms against the reference's run. The device
+    FP64 forces differ from the reference's at round-off (summation order), so the trajectories agree to
+    the VelocityVerlet trajectory test's 1e-9, not bitwise; the report gains its thermostat rows."""
+    from devinproj_b200 import Langevin, LennardJones, NoseHoover, Simulation
+    g = golden("thermostats108")
+    s = product_system(g, "0")
+    lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
+    integ = Langevin(float(g["T"]), float(g["friction"])) if kind == "lv" else NoseHoover(float(g["T"]), float(g["tau"]))
+    sim = Simulation(s, [lj], integrator=integ, dt=float(g["dt"]), seed=int(g["seed"]))
+    tr = sim.run(steps=int(g["steps"]), record_every=int(g["record_every"]), positions=False)
+    d = s.pos - g[f"{kind}_pos"]
+    d -= s.box * np.round(d / s.box)
+    assert np.max(np.abs(d)) <= 1e-9 * s.box[0]
+    assert rel_max(s.vel, g[f"{kind}_vel"]) <= 1e-9
+    assert rel_max(np.array(tr.kinetic), g[f"{kind}_kinetic"]) <= 1e-9
+    assert rel_max(np.array(tr.potential), g[f"{kind}_potential"]) <= 1e-9
+    if kind == "nh":
+        assert rel_max(np.array(tr.bath), g["nh_bath"]) <= 1e-9
+        assert abs(integ.xi - g["nh_xi"]) <= 1e-9 * abs(g["nh_xi"]) and integ.Q == g["nh_Q"]
+    rows = {c.name for c in sim.accuracy_report().checks}
+    assert "thermostat" in rows and (("extended energy" in rows) == (kind == "nh"))
+
+
+def test_langevin_o_step_is_bit_identical():
+    """Given the same velocities, per-atom sigma and normal draws, acs_langevin_ou computes the reference's
+    c1 * v + sig * noise exactly (accusim/integrators.py:66-67)."""
+    import torch
+
+    from devinproj_b200 import _lib
+    from devinproj_b200.device import stream_handle, to_dev
+    rng = np.random.default_rng(5)
+    n = 1000
+    vel = rng.normal(size=(n, 3)) * 300.0
+    noise = rng.normal(size=(n, 3))
+    masses = rng.choice([6.6e-26, 1.4e-25], n)
+    c1 = np.exp(-5e12 * 5e-15)
+    sig = np.sqrt((1 - c1 ** 2) * 1.380649e-23 * 120.0 / masses)
+    ref = c1 * vel + sig[:, None] * noise
+    L = _lib.lib()
+    v, z, sg = to_dev(vel), to_dev(noise), to_dev(sig)   # held: a freed temporary's memory is handed out again
+    _lib.check(L.acs_langevin_ou(v.data_ptr(), z.data_ptr(), sg.data_ptr(), n, float(c1), stream_handle()))
+    torch.cuda.synchronize()
+    assert np.array_equal(v.cpu().numpy(), ref)

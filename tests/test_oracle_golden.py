@@ -119,3 +119,24 @@ def test_oracle_known_answer_lj_minimum():
     st = port.State(pos, np.zeros_like(pos), np.zeros(2, int), np.arange(2), None, False, [("Ar", 6.6e-26, 0.0)])
     F, _ = port.LennardJones({"Ar": (1e-21, sigma)}, cutoff=10).compute(st)
     assert np.allclose(F, 0, atol=1e-20)
+
+
+@pytest.mark.parametrize("kind", ["lv", "nh"])
+def test_oracle_thermostats_match_reference(golden, kind):
+    """Langevin BAOAB (the reference's draws: default_rng(seed).normal) and Nose-Hoover on 108 argon atoms,
+    40 steps: bit-identical to the reference's run."""
+    g = golden("thermostats108")
+    st = oracle_state(g, "0")
+    lj = port.LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
+    if kind == "lv":
+        rng = np.random.default_rng(int(g["seed"]))
+        integ = port.LangevinBAOAB(float(g["T"]), float(g["friction"]), lambda shape: rng.normal(size=shape))
+    else:
+        integ = port.NoseHooverMTK(float(g["T"]), float(g["tau"]))
+    run = port.Run(st, [lj], float(g["dt"]), integrator=integ).run(int(g["steps"]), int(g["record_every"]))
+    assert np.array_equal(st.pos, g[f"{kind}_pos"]) and np.array_equal(st.vel, g[f"{kind}_vel"])
+    assert np.array_equal(np.array(run.kinetic), g[f"{kind}_kinetic"])
+    assert np.array_equal(np.array(run.potential), g[f"{kind}_potential"])
+    assert np.array_equal(np.array(run.bath), g[f"{kind}_bath"])
+    if kind == "nh":
+        assert integ.xi == g["nh_xi"] and integ.eta == g["nh_eta"] and integ.Q == g["nh_Q"]
