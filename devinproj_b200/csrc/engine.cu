@@ -53,6 +53,8 @@ struct RepDev {
   float csf[3];
   float pad0;
   double dt, hdt, hs2, rl2;
+  double lv_c1, lv_pad;                 // Langevin: exp(-gamma dt)
+  double lv_sig[ACS_MAX_SPECIES];       // Langevin: sqrt((1 - c1^2) kT / m) per species
 };
 
 struct FFDev {
@@ -93,7 +95,47 @@ struct Eng {
   unsigned int* bar;  // [0] counter, [1] generation
   unsigned long long* phase_ns;  // rebuild phase durations, accumulated (block 0 timestamps)
   const float* fext;             // optional per-slot force added to the pair forces (learned correction)
+  int32_t thermo;                // 0 VelocityVerlet, 1 Langevin BAOAB
+  uint32_t seed_lo, seed_hi;
+  unsigned long long* octr;      // O-steps taken so far (Langevin draws: counter)
 };
+
+// ------------------------------------------------------------------- Langevin normal draws --
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011): ten rounds of two 32x32->64-bit products with the
+// published multipliers, the key bumped by the Weyl constants between rounds.
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+  }
+}
+
+// Three standard normals (Box-Muller on u = (x + 1/2) 2^-32) for one atom and one O-step.
+__device__ __forceinline__ void langevin_normals(const Eng& E, unsigned long long ostep, int32_t id, int32_t rep,
+                                                 double z[3]) {
+  uint32_t c[4] = {(uint32_t)ostep, (uint32_t)(ostep >> 32), (uint32_t)id, (uint32_t)rep};
+  philox4x32_10(c, E.seed_lo, E.seed_hi);
+  const double s32 = 2.3283064365386963e-10;  // 2^-32
+  const double u0 = ((double)c[0] + 0.5) * s32, u1 = ((double)c[1] + 0.5) * s32;
+  const double u2 = ((double)c[2] + 0.5) * s32, u3 = ((double)c[3] + 0.5) * s32;
+  const double r0 = sqrt(-2.0 * log(u0)), r1 = sqrt(-2.0 * log(u2));
+  double s0, c0, s1, c1;
+  sincospi(2.0 * u1, &s0, &c0);
+  sincospi(2.0 * u3, &s1, &c1);
+  z[0] = r0 * c0;
+  z[1] = r0 * s0;
+  z[2] = r1 * c1;
+}
 
 __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
@@ -241,8 +283,34 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
 // A warp handles G = 32/tpa atoms; the tpa lanes of an atom split its neighbour list (lane = phase*G +
 // atom-in-group, so each batch of list reads is one coalesced 128-byte row) and their Kahan partial sums
 // are combined in FP64 by a fixed xor-shuffle tree (deterministic).
-template <bool LJ, bool DSF, bool REC, int MODE, bool ONE>
-__global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int dst) {
+// Second half of a step's start after the first kick: drift (VelocityVerlet), or half drift, the
+// Ornstein-Uhlenbeck velocity update and half drift (BAOAB) with the draws of O-step *octr + ostep.
+template <bool LV>
+__device__ __forceinline__ void drift_or_baoab(const Eng& E, const RepDev& R, int64_t i, int r, int si,
+                                               unsigned ostep, double& vx, double& vy, double& vz, double& ux,
+                                               double& uy, double& uz) {
+  if (LV) {
+    ux = E.u[3 * i] + R.hdt * vx;
+    uy = E.u[3 * i + 1] + R.hdt * vy;
+    uz = E.u[3 * i + 2] + R.hdt * vz;
+    double z[3];
+    langevin_normals(E, *E.octr + ostep, E.id[i], r, z);
+    const double sg = R.lv_sig[si];
+    vx = R.lv_c1 * vx + sg * z[0];
+    vy = R.lv_c1 * vy + sg * z[1];
+    vz = R.lv_c1 * vz + sg * z[2];
+    ux += R.hdt * vx;
+    uy += R.hdt * vy;
+    uz += R.hdt * vz;
+  } else {
+    ux = E.u[3 * i] + R.dt * vx;
+    uy = E.u[3 * i + 1] + R.dt * vy;
+    uz = E.u[3 * i + 2] + R.dt * vz;
+  }
+}
+
+template <bool LJ, bool DSF, bool REC, int MODE, bool ONE, bool LV = false>
+__global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int dst, unsigned ostep) {
   __shared__ float4 shift_tab[8][27];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
@@ -365,7 +433,8 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         vx += R.hdt * ax;
         vy += R.hdt * ay;
         vz += R.hdt * az;
-        const double ux = E.u[3 * i] + R.dt * vx, uy = E.u[3 * i + 1] + R.dt * vy, uz = E.u[3 * i + 2] + R.dt * vz;
+        double ux, uy, uz;
+        drift_or_baoab<LV>(E, R, i, r, si, ostep, vx, vy, vz, ux, uy, uz);
         E.u[3 * i] = ux;
         E.u[3 * i + 1] = uy;
         E.u[3 * i + 2] = uz;
@@ -395,6 +464,9 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
   }
 }
 
+// End of a block of `steps` steps: the Langevin draws of the next block continue the O-step count.
+__global__ void k_octr_advance(unsigned long long* octr, int steps) { *octr += (unsigned long long)steps; }
+
 // Prologue of a block: first half-kick and drift from the stored accelerations, image, skin test.
 __global__ void k_prologue(Eng E, int dst) {
   if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
@@ -406,7 +478,9 @@ __global__ void k_prologue(Eng E, int dst) {
     double vx = E.v[3 * i] + R.hdt * E.acc[3 * i];
     double vy = E.v[3 * i + 1] + R.hdt * E.acc[3 * i + 1];
     double vz = E.v[3 * i + 2] + R.hdt * E.acc[3 * i + 2];
-    const double ux = E.u[3 * i] + R.dt * vx, uy = E.u[3 * i + 1] + R.dt * vy, uz = E.u[3 * i + 2] + R.dt * vz;
+    double ux, uy, uz;
+    if (E.thermo == 1) drift_or_baoab<true>(E, R, i, r, E.sp[i], 0u, vx, vy, vz, ux, uy, uz);
+    else drift_or_baoab<false>(E, R, i, r, E.sp[i], 0u, vx, vy, vz, ux, uy, uz);
     E.v[3 * i] = vx;
     E.v[3 * i + 1] = vy;
     E.v[3 * i + 2] = vz;
@@ -1275,6 +1349,11 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
   }
   const int G = 32 / tpa;
   err = ACS_OK;
+  if (cfg->thermo.kind < 0 || cfg->thermo.kind > 1 ||
+      (cfg->thermo.kind == 1 && !(cfg->thermo.kT >= 0.0 && cfg->thermo.friction >= 0.0))) {
+    err = ACS_ERR_ARG;
+    return;
+  }
   reps.clear();
   src0.clear();
   S = 0;
@@ -1325,6 +1404,11 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     R.hdt = 0.5 * q.dt;
     R.hs2 = q.half_skin * q.half_skin;
     R.rl2 = q.rlist * q.rlist;
+    if (cfg->thermo.kind == 1) {  // accusim/integrators.py:65-66
+      R.lv_c1 = exp(-cfg->thermo.friction * q.dt);
+      for (int t = 0; t < cfg->ff.n_species && t < ACS_MAX_SPECIES; ++t)
+        R.lv_sig[t] = sqrt((1.0 - R.lv_c1 * R.lv_c1) * cfg->thermo.kT / cfg->ff.mass[t]);
+    }
     reps.push_back(R);
     src0.push_back(g);
     g += q.n;
@@ -1384,6 +1468,7 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(4 * (size_t)NCC);                    // 39 cc_sum
   L.add(8 * 16);                             // 40 phase timers
   L.add(4 * (size_t)S);                      // 41 perm2
+  L.add(8);                                  // 42 Langevin O-step counter
   return L;
 }
 
@@ -1433,30 +1518,34 @@ FFDev make_ff(const acs_forcefield& f, int& err) {
 }
 
 template <bool LJ, bool DSF, bool ONE>
-int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
+int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, unsigned ostep, cudaStream_t s) {
   dim3 g(e->step_blocks), b(e->step_threads);
-  if (mode == 0) {
-    if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
-    else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+  if (mode == 0 && e->E.thermo == 1) {
+    if (rec) k_step<LJ, DSF, true, 0, ONE, true><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    else k_step<LJ, DSF, false, 0, ONE, true><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+  } else if (mode == 0) {
+    if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
   } else if (mode == 1) {
-    if (rec) k_step<LJ, DSF, true, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
-    else k_step<LJ, DSF, false, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    if (rec) k_step<LJ, DSF, true, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    else k_step<LJ, DSF, false, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
   } else {
-    k_step<LJ, DSF, true, 2, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst);
+    k_step<LJ, DSF, true, 2, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
   }
   return launch_status();
 }
 
-int launch_step(acs_engine* e, int rec, int mode, int src, int dst, cudaStream_t s) {
+// ostep: offset of the O-step this launch's BAOAB takes, from the counter's value at the block start.
+int launch_step(acs_engine* e, int rec, int mode, int src, int dst, unsigned ostep, cudaStream_t s) {
   const bool one = e->ff.ns == 1;
   if (e->ff.lj && e->ff.dsf)
-    return one ? launch_step_t<true, true, true>(e, rec, mode, src, dst, s)
-               : launch_step_t<true, true, false>(e, rec, mode, src, dst, s);
+    return one ? launch_step_t<true, true, true>(e, rec, mode, src, dst, ostep, s)
+               : launch_step_t<true, true, false>(e, rec, mode, src, dst, ostep, s);
   if (e->ff.lj)
-    return one ? launch_step_t<true, false, true>(e, rec, mode, src, dst, s)
-               : launch_step_t<true, false, false>(e, rec, mode, src, dst, s);
-  return one ? launch_step_t<false, true, true>(e, rec, mode, src, dst, s)
-             : launch_step_t<false, true, false>(e, rec, mode, src, dst, s);
+    return one ? launch_step_t<true, false, true>(e, rec, mode, src, dst, ostep, s)
+               : launch_step_t<true, false, false>(e, rec, mode, src, dst, ostep, s);
+  return one ? launch_step_t<false, true, true>(e, rec, mode, src, dst, ostep, s)
+             : launch_step_t<false, true, false>(e, rec, mode, src, dst, ostep, s);
 }
 
 // Descriptors + tensor-core MLP -> per-slot correction forces for the images in buffer `src`.
@@ -1498,11 +1587,15 @@ int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cud
     const bool last = (k == steps - 1);
     const int rec = rec_at[k] ? 1 : 0;
     if (k % e->c_stride == 0 && (st = launch_correction(e, src, s))) return st;
-    if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, s))) return st;
+    if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, (unsigned)(k + 1), s))) return st;
     if (!last || rec) {
       if ((st = launch_rebuild(e, dst, rec, rec_idx, 0, s))) return st;
     }
     rec_idx += rec;
+  }
+  if (e->E.thermo) {
+    k_octr_advance<<<1, 1, 0, s>>>(e->E.octr, steps);
+    return launch_status();
   }
   return ACS_OK;
 }
@@ -1606,6 +1699,10 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.cc_sum = (int32_t*)(b + L.off[39]);
   E.phase_ns = (unsigned long long*)(b + L.off[40]);
   E.perm2 = (int32_t*)(b + L.off[41]);
+  E.octr = (unsigned long long*)(b + L.off[42]);
+  E.thermo = cfg->thermo.kind;
+  E.seed_lo = (uint32_t)cfg->thermo.seed;
+  E.seed_hi = (uint32_t)(cfg->thermo.seed >> 32);
 
   // host-built index tables
   std::vector<int32_t> tile_rep(T), cell_rep(C), chunk_rep(NCH), chunk_t0(NCH), chunk_nt(NCH);
@@ -1647,6 +1744,7 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   ok = ok && cudaMemcpy(E.cc_n, cc_n.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemset(E.nnb, 0, 4 * (size_t)S) == cudaSuccess;
   ok = ok && cudaMemset(E.phase_ns, 0, 8 * 16) == cudaSuccess;
+  ok = ok && cudaMemset(E.octr, 0, 8) == cudaSuccess;
   int sms = 0, per_sm = 0;
   ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev) == cudaSuccess;
   ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, 256, 0) == cudaSuccess;
@@ -1672,7 +1770,7 @@ int acs_engine_set_state(acs_engine* e, const double* pos, const double* vel, co
   // build lists for every replica, then one force evaluation (accelerations + initial records)
   if ((st = launch_rebuild(e, 0, 0, 0, 1, s))) return st;
   if ((st = launch_correction(e, 0, s))) return st;
-  if ((st = launch_step(e, 1, 2, 0, 0, s))) return st;
+  if ((st = launch_step(e, 1, 2, 0, 0, 0u, s))) return st;
   return launch_rebuild(e, 0, 1, 0, 0, s);
 }
 
@@ -1824,9 +1922,13 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
     const bool last = (k == steps - 1);
     const int rec = ((record_every > 0 && (k + 1) % record_every == 0) || last) ? 1 : 0;
     if (e->corr && k % e->c_stride == 0) st = mark(2, [&] { return launch_correction(e, src, s); });
-    if (!st) st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, s); });
+    if (!st) st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, (unsigned)(k + 1), s); });
     if (!st) st = mark(1, [&] { return launch_rebuild(e, dst, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, 0, s); });
     rec_idx += rec;
+  }
+  if (!st && e->E.thermo) {
+    k_octr_advance<<<1, 1, 0, s>>>(e->E.octr, steps);
+    st = launch_status();
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) st = ACS_ERR_CUDA;
   float tot[3] = {0.f, 0.f, 0.f};

@@ -19,7 +19,7 @@ import torch
 
 from . import _lib
 from .device import require_cuda, stream_handle, to_dev
-from .units import N_A, amu, e_charge, k_e
+from .units import N_A, amu, e_charge, k_B, k_e
 
 LEN = 1e-10
 MASS = amu
@@ -45,9 +45,23 @@ class ForceField(C.Structure):
                 ("dsf_k", C.c_double), ("q", C.c_double * 8)]
 
 
+class Thermostat(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("pad", C.c_int32), ("kT", C.c_double), ("friction", C.c_double),
+                ("seed", C.c_uint64)]
+
+
 class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
-                ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField)]
+                ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
+                ("thermo", Thermostat)]
+
+
+def langevin_thermostat(integrator, seed):
+    """Engine thermostat block for a Langevin integrator (this package's or the reference's; SI T and
+    friction) in engine units; seed None draws one."""
+    if seed is None:
+        seed = int(np.random.default_rng().integers(2 ** 63))
+    return Thermostat(1, 0, k_B * float(integrator.T) / ENERGY, float(integrator.gamma) * TIME, int(seed) % 2 ** 64)
 
 
 class DevStatusC(C.Structure):
@@ -132,7 +146,8 @@ class _SpeciesView:
 class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
-    def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1):
+    def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
+                 thermo=None):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -149,7 +164,8 @@ class Engine:
             self._reps[k].rlist = float(r["rlist"])
             self._reps[k].half_skin = float(r["half_skin"])
         self.tpa = int(tpa)
-        self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff)
+        self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff,
+                                thermo if thermo is not None else Thermostat())
         nbytes = L.acs_engine_bytes(C.byref(self.cfg))
         if nbytes == 0:
             raise ValueError("engine configuration rejected (sizes, list radius >= box/2, or too many replicas)")
@@ -303,7 +319,7 @@ def default_tpa(n_atoms_total, neighbors_per_atom):
     return tpa
 
 
-def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None):
+def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -314,7 +330,7 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
         maxnb = expect
     if tpa is None:
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3)
-    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa), rlist, half_skin
+    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo), rlist, half_skin
 
 
 def _upload_state(engine, systems):
@@ -330,7 +346,7 @@ def _upload_state(engine, systems):
     engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
 
 
-def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None):
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None):
     """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
     grows the neighbour capacity once if the first build overflows."""
     for s in systems:
@@ -343,7 +359,7 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=
     reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
     for attempt in range(3):
         eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,
-                                      tpa=tpa)
+                                      tpa=tpa, thermo=thermo)
         _upload_state(eng, systems)
         st = eng.status()
         if st.flags & _lib.FLAG_OVERFLOW:
@@ -362,8 +378,8 @@ class GpuSimulation:
     """`Simulation` with the step loop on the device (accusim/simulation.py:40-131 interface).
 
     forces: [LennardJones] and/or [DampedShiftedCoulomb] (this package's or the reference's classes);
-    integrator: VelocityVerlet only. `system.pos`/`vel` are synchronised from the device after every
-    `run` call (and at records when positions=True)."""
+    integrator: VelocityVerlet, or Langevin (BAOAB, counter-based draws keyed by `seed`). `system.pos`/`vel`
+    are synchronised from the device after every `run` call (and at records when positions=True)."""
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
                  rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500, correction_stride=1):
@@ -372,8 +388,10 @@ class GpuSimulation:
         from .units import si
         if reactions:
             raise NotImplementedError("reactions are not part of the accusim_b200 force-and-step path")
-        if integrator is not None and type(integrator).__name__ != "VelocityVerlet":
-            raise ValueError("GpuSimulation integrates with VelocityVerlet")
+        kind = type(integrator).__name__ if integrator is not None else "VelocityVerlet"
+        if kind not in ("VelocityVerlet", "Langevin"):
+            raise ValueError("GpuSimulation integrates with VelocityVerlet or Langevin (BAOAB)")
+        thermo = langevin_thermostat(integrator, seed) if kind == "Langevin" else None
         self.system = system
         self.forces = list(forces)
         self.integrator = integrator or VelocityVerlet()
@@ -387,7 +405,7 @@ class GpuSimulation:
         self._initial = None
         self.engine, self.rlist, self.half_skin = start_engine(
             [system], self.forces, [self.dt if self.dt is not None else 1e-15], maxnb=maxnb, rec_cap=rec_cap,
-            grid_mult=grid_mult, tpa=tpa)
+            grid_mult=grid_mult, tpa=tpa, thermo=thermo)
         self.correction = None
         self.validate_every = int(validate_every)
         self.validations = []

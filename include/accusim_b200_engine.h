@@ -41,6 +41,19 @@ typedef struct acs_forcefield {
   double q[8];        /* charge per species */
 } acs_forcefield;
 
+/* Thermostat of the engine's step. kind 0: VelocityVerlet (accusim/integrators.py:25-31); kind 1:
+ * Langevin BAOAB (accusim/integrators.py:50-71) with c1 = exp(-friction dt) and sigma = sqrt((1 - c1^2)
+ * kT / m) per species and replica. Its standard normal draws are counter-based (Philox4x32-10, key = seed,
+ * counter = (O-step index, atom index within the replica, replica)), so a run is reproducible and does
+ * not depend on list rebuilds or on which other replicas share the engine. */
+typedef struct acs_thermostat {
+  int32_t kind;
+  int32_t pad;
+  double kT;          /* k_B T in the caller's energy unit */
+  double friction;    /* gamma, in 1 / caller time unit */
+  uint64_t seed;
+} acs_thermostat;
+
 typedef struct acs_engine_config {
   int32_t n_replicas;
   int32_t maxnb;      /* neighbour capacity per atom */
@@ -50,6 +63,7 @@ typedef struct acs_engine_config {
   int32_t pad;
   const acs_replica* replicas;  /* host array */
   acs_forcefield ff;
+  acs_thermostat thermo;        /* zero: VelocityVerlet */
 } acs_engine_config;
 
 typedef struct acs_engine acs_engine;

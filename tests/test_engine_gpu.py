@@ -196,3 +196,51 @@ def test_dense_cells_lists_match_oracle(tpa):
                                                                    skin=0.0)))
     masses = np.array([x.mass for x in s.species])[s.sp][:, None]
     assert rms_rel(a.cpu().numpy() * ACC * masses, Fo) <= 1e-5
+
+
+def test_engine_langevin_matches_oracle_with_the_same_draws():
+    """BAOAB inside the engine (fused into the step kernel, counter-based Philox draws) against the FP64
+    oracle's BAOAB fed the same draws (oracle/philox.py): 10 steps of the 864-atom argon case. Positions
+    agree to FP32-force level (1e-9 of the box), velocities to 1e-6."""
+    from devinproj_b200 import GpuSimulation, Langevin, configs
+    from oracle import philox
+    s, forces, dt = configs.argon864(seed=2)
+    st = oracle_of(s)
+    seed = 987654321
+    sim = GpuSimulation(s, forces, integrator=Langevin(120.0, 5e12), dt=dt, seed=seed)
+    sim.run(steps=10, record_every=5, positions=False)
+    j = [0]
+
+    def draws(shape):
+        z = philox.normals(j[0], np.arange(shape[0]), 0, seed)
+        j[0] += 1
+        return z
+    lj = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)
+    port.Run(st, [lj], dt, integrator=port.LangevinBAOAB(120.0, 5e12, draws)).run(10)
+    d = s.pos - st.pos
+    d -= s.box * np.round(d / s.box)
+    assert np.max(np.abs(d)) <= 1e-9 * s.box[0]
+    assert rel_max(s.vel, st.vel) <= 1e-6
+
+
+def test_engine_langevin_thermostats_and_zero_friction_is_verlet():
+    """A 2000-step Langevin run from 60 K reaches the 120 K target (the report's thermostat row passes), and
+    with zero friction the BAOAB step is VelocityVerlet: two half drifts round differently from one full
+    drift, and a flipped FP32 image rounding moves forces by ~1e-7, so the 50-step trajectories agree to
+    1e-9 of the box."""
+    from devinproj_b200 import GpuSimulation, Langevin, VelocityVerlet, configs
+    s, forces, dt = configs.argon864(seed=4)
+    s.vel *= np.sqrt(60.0 / s.temperature())
+    sim = GpuSimulation(s, forces, integrator=Langevin(120.0, 2e12), dt=dt, seed=7)
+    sim.run(steps=2000, record_every=50, positions=False)
+    row = {c.name: c for c in sim.accuracy_report().checks}["thermostat"]
+    assert row.status == "PASS", row
+    s1, forces1, _ = configs.argon864(seed=5)
+    s2 = s1.copy()
+    a = GpuSimulation(s1, forces1, integrator=Langevin(120.0, 0.0), dt=dt, seed=1)
+    b = GpuSimulation(s2, forces1, integrator=VelocityVerlet(), dt=dt)
+    a.run(steps=50, record_every=50, positions=False)
+    b.run(steps=50, record_every=50, positions=False)
+    d = s1.pos - s2.pos
+    d -= s1.box * np.round(d / s1.box)
+    assert np.max(np.abs(d)) <= 1e-9 * s1.box[0]

@@ -140,3 +140,17 @@ def test_oracle_thermostats_match_reference(golden, kind):
     assert np.array_equal(np.array(run.bath), g[f"{kind}_bath"])
     if kind == "nh":
         assert integ.xi == g["nh_xi"] and integ.eta == g["nh_eta"] and integ.Q == g["nh_Q"]
+
+
+def test_philox_known_answers():
+    """The oracle's Philox4x32-10 (the engine's Langevin draws) reproduces the published known-answer vectors
+    of the algorithm (Random123 distribution, kat_vectors: philox4x32, 10 rounds)."""
+    from oracle.philox import normals, philox4x32_10
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+             ((0xffffffff,) * 4, (0xffffffff, 0xffffffff), (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+             ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+              (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for ctr, key, out in cases:
+        assert tuple(int(v) for v in philox4x32_10(np.array([ctr], np.uint64), key)[0]) == out
+    z = normals(3, np.arange(200000), 0, 12345)
+    assert abs(z.mean()) < 0.01 and abs(z.std() - 1.0) < 0.01
