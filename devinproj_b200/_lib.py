@@ -47,6 +47,8 @@ SIGNATURES = {
     "acs_dsf_fp64": (C.c_int, [P, P, I64, P, C.c_int, P, P, I32, P, P, DBL, DBL, DBL, P, P, P, SZ, P]),
     "acs_vv_kick": (C.c_int, [P, P, I64, DBL, P]),
     "acs_langevin_ou": (C.c_int, [P, P, P, I64, DBL, P]),
+    "acs_rdf_work_bytes": (SZ, [I64, P]),
+    "acs_rdf_hist": (C.c_int, [P, P, I64, P, I32, I32, DBL, P, P, SZ, P]),
     "acs_vv_drift_wrap": (C.c_int, [P, P, I64, DBL, P, C.c_int, P]),
     "acs_vv_accel": (C.c_int, [P, P, P, P, I32, I64, P]),
     "acs_reduce_work_bytes": (SZ, [I64]),

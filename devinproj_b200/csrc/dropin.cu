@@ -207,6 +207,58 @@ __global__ void k_list(const double* __restrict__ pos, int64_t n, GridDev g, con
   }
 }
 
+// Pair-distance histogram of accusim/analysis.py:7-24 (rdf): pairs i < j, both of `species` (all when < 0),
+// minimum-image r by the reference's FP64 expression, binned by NumPy's uniform-bin rule on [0, rmax]
+// (numpy histogram: index = int((r / rmax) * bins), the right edge into the last bin, then one step down if
+// r < edge[index] or up if r >= edge[index + 1] below the last bin, with edge[k] = k * (rmax / bins) and
+// edge[bins] = rmax). Per-block shared-memory counts, integer atomics: exact and order-independent.
+__global__ void k_rdf(const double* __restrict__ pos, const int32_t* __restrict__ sp, int64_t n, GridDev g,
+                      const int32_t* __restrict__ cell_of, const int32_t* __restrict__ start,
+                      const int32_t* __restrict__ cell_atoms, int species, int bins, double rmax, double step,
+                      unsigned long long* __restrict__ hist) {
+  extern __shared__ unsigned int sh_hist[];
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) sh_hist[b] = 0u;
+  __syncthreads();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && (species < 0 || sp[i] == species)) {
+    const int c = cell_of[i];
+    const int c2 = c % g.nc[2], c1 = (c / g.nc[2]) % g.nc[1], c0 = c / (g.nc[2] * g.nc[1]);
+    const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+    int lo0, hi0, lo1, hi1, lo2, hi2;
+    stencil_range(c0, g.nc[0], g.box.periodic, lo0, hi0);
+    stencil_range(c1, g.nc[1], g.box.periodic, lo1, hi1);
+    stencil_range(c2, g.nc[2], g.box.periodic, lo2, hi2);
+    for (int a = lo0; a <= hi0; ++a) {
+      const int n0 = wrap_cell(c0 + a, g.nc[0]);
+      for (int b = lo1; b <= hi1; ++b) {
+        const int n1 = wrap_cell(c1 + b, g.nc[1]);
+        for (int d = lo2; d <= hi2; ++d) {
+          const int n2 = wrap_cell(c2 + d, g.nc[2]);
+          const int nb = (n0 * g.nc[1] + n1) * g.nc[2] + n2;
+          for (int k = start[nb], e = start[nb + 1]; k < e; ++k) {
+            const int j = cell_atoms[k];
+            if (j <= i || (species >= 0 && sp[j] != species)) continue;
+            double dx = sub(pos[3 * (int64_t)j], xi), dy = sub(pos[3 * (int64_t)j + 1], yi),
+                   dz = sub(pos[3 * (int64_t)j + 2], zi);
+            min_image3(dx, dy, dz, g.box);
+            const double r = __dsqrt_rn(norm2(dx, dy, dz));
+            if (!(r <= rmax)) continue;
+            int idx = (int)mul(__ddiv_rn(r, rmax), (double)bins);
+            if (idx == bins) idx -= 1;
+            if (r < mul((double)idx, step)) idx -= 1;
+            const double upper = idx + 1 == bins ? rmax : mul((double)(idx + 1), step);
+            if (r >= upper && idx != bins - 1) idx += 1;
+            atomicAdd(&sh_hist[idx], 1u);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < bins; b += blockDim.x)
+    if (sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)sh_hist[b]);
+}
+
 __global__ void k_pairs(const int32_t* __restrict__ nbr, const int32_t* __restrict__ nnb, int64_t n, int maxnb,
                         int32_t* pi, int32_t* pj, int64_t cap, unsigned long long* count) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -424,6 +476,35 @@ double py_floordiv(double a, double b) {
   return fl;
 }
 
+constexpr int kRdfMaxBins = 8192;   // shared-memory counts per block
+
+// Cell binning shared by the list build and the pair histogram: atoms counted into cells, exclusive scan,
+// scatter, deterministic in-cell order (ascending atom index).
+struct CellBins {
+  int32_t *cell_of, *start, *cell_atoms;
+};
+int bin_cells(const double* pos, int64_t n, const acs_grid* g, void* work, cudaStream_t s, CellBins& cb) {
+  const int64_t nc = grid_cells(g);
+  const int64_t nchunks = ceil_div(nc + 1, kScanChunk);
+  char* w = (char*)work;
+  cb.cell_of = (int32_t*)w; w += align256(n * 4);
+  int32_t* count = (int32_t*)w; w += align256((nc + 1) * 4);
+  cb.start = (int32_t*)w; w += align256((nc + 1) * 4);
+  cb.cell_atoms = (int32_t*)w; w += align256(n * 4);
+  int32_t* sums = (int32_t*)w;
+  GridDev gd = to_dev(g);
+  if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return 1;
+  const int nb = (int)ceil_div(n, kBlock);
+  k_bin<<<nb, kBlock, 0, s>>>(pos, n, gd, cb.cell_of, count);
+  k_scan_chunks<<<(int)nchunks, kScanThreads, 0, s>>>(count, cb.start, nc + 1, sums);
+  k_scan_sums<<<1, kScanThreads, 0, s>>>(sums, nchunks, nullptr);
+  k_scan_add<<<(int)nchunks, 256, 0, s>>>(cb.start, nc + 1, sums);
+  if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return 1;
+  k_scatter<<<nb, kBlock, 0, s>>>(cb.cell_of, n, cb.start, count, cb.cell_atoms);
+  k_sort_cells<<<(int)ceil_div(nc, kBlock), kBlock, 0, s>>>(cb.start, nc, cb.cell_atoms);
+  return 0;
+}
+
 }  // namespace
 
 // ===================================================================================== C ABI ==
@@ -501,23 +582,29 @@ int acs_nlist_build(const double* pos, int64_t n, const acs_grid* g, int32_t max
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t nc = grid_cells(g);
   const int64_t nchunks = ceil_div(nc + 1, kScanChunk);
-  char* w = (char*)work;
-  int32_t* cell_of = (int32_t*)w; w += align256(n * 4);
-  int32_t* count = (int32_t*)w; w += align256((nc + 1) * 4);
-  int32_t* start = (int32_t*)w; w += align256((nc + 1) * 4);
-  int32_t* cell_atoms = (int32_t*)w; w += align256(n * 4);
-  int32_t* sums = (int32_t*)w;
-  GridDev gd = to_dev(g);
-  if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return ACS_ERR_CUDA;
-  const int nb = (int)ceil_div(n, kBlock);
-  k_bin<<<nb, kBlock, 0, s>>>(pos, n, gd, cell_of, count);
-  k_scan_chunks<<<(int)nchunks, kScanThreads, 0, s>>>(count, start, nc + 1, sums);
-  k_scan_sums<<<1, kScanThreads, 0, s>>>(sums, nchunks, nullptr);
-  k_scan_add<<<(int)nchunks, 256, 0, s>>>(start, nc + 1, sums);
-  if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return ACS_ERR_CUDA;
-  k_scatter<<<nb, kBlock, 0, s>>>(cell_of, n, start, count, cell_atoms);
-  k_sort_cells<<<(int)ceil_div(nc, kBlock), kBlock, 0, s>>>(start, nc, cell_atoms);
-  k_list<<<nb, kBlock, 0, s>>>(pos, n, gd, cell_of, start, cell_atoms, maxnb, nbr, nnb, status);
+  CellBins cb;
+  if (bin_cells(pos, n, g, work, s, cb)) return ACS_ERR_CUDA;
+  k_list<<<(int)ceil_div(n, kBlock), kBlock, 0, s>>>(pos, n, to_dev(g), cb.cell_of, cb.start, cb.cell_atoms, maxnb,
+                                                     nbr, nnb, status);
+  return launch_status();
+}
+
+size_t acs_rdf_work_bytes(int64_t n, const acs_grid* g) { return acs_nlist_work_bytes(n, g); }
+
+int acs_rdf_hist(const double* pos, const int32_t* sp, int64_t n, const acs_grid* g, int32_t species, int32_t bins,
+                 double rmax, unsigned long long* hist, void* work, size_t work_bytes, void* stream) {
+  if (!g || n < 0 || n > INT32_MAX || bins < 1 || bins > kRdfMaxBins || !(rmax > 0.0) || !hist ||
+      (n > 0 && (!pos || !work || (species >= 0 && !sp))))
+    return ACS_ERR_ARG;
+  if (!g->periodic || !(g->rc >= rmax)) return ACS_ERR_ARG;   // cells no narrower than rmax, periodic box
+  if (work_bytes < acs_rdf_work_bytes(n, g)) return ACS_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * bins, s) != cudaSuccess) return ACS_ERR_CUDA;
+  if (n == 0) return ACS_OK;
+  CellBins cb;
+  if (bin_cells(pos, n, g, work, s, cb)) return ACS_ERR_CUDA;
+  k_rdf<<<(int)ceil_div(n, kBlock), kBlock, sizeof(unsigned int) * bins, s>>>(
+      pos, sp, n, to_dev(g), cb.cell_of, cb.start, cb.cell_atoms, species, bins, rmax, rmax / bins, hist);
   return launch_status();
 }
 

@@ -200,17 +200,19 @@ def rms_rel(F, Fref):
 def generate_dataset(n_snapshots, seed=0, n_sites=20, T=1300.0, melt_T=4000.0, melt_steps=2000, equil_steps=2000,
                      interval=20, rcut=10e-10, alpha=0.2e10, verbose=False):
     """Snapshots of a NaCl melt (LJ + DSF, FP32-compensated engine) with labels F_Ewald - F_DSF (SI, FP64,
-    device Ewald with the reference's default parameters). Returns a dict of host arrays."""
+    device Ewald with the reference's default parameters). As the reference's molten-salt example does
+    (examples/molten_salt.py:38-44): Langevin melting at `melt_T`, Langevin cooling to T (friction 5/ps),
+    then NVE sampling every `interval` steps. Returns a dict of host arrays."""
     from . import configs
     from .engine import GpuSimulation
     from .ewald import Ewald
+    from .integrators import Langevin
     s, forces = configs.nacl_melt(n_sites, T=melt_T, rcut=rcut, alpha=alpha, seed=seed)
     dt = 1e-15
+    for temp, steps in ((melt_T, melt_steps), (T, equil_steps)):
+        GpuSimulation(s, forces, integrator=Langevin(temp, 5e12), dt=dt, seed=seed).run(
+            steps=steps, record_every=steps, positions=False)
     sim = GpuSimulation(s, forces, dt=dt)
-    sim.run(steps=melt_steps, record_every=melt_steps, positions=False)
-    s.vel *= math.sqrt(T / max(s.temperature(), 1.0))
-    sim.update_forces()          # re-uploads the rescaled host state
-    sim.run(steps=equil_steps, record_every=equil_steps, positions=False)
     ew = Ewald(k=forces[1].k)
     dsf = forces[1]
     pos, sp, res, fd = [], [], [], []

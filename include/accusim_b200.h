@@ -14,6 +14,7 @@
  *   acs_dsf_fp64                 accusim/forces.py:408-452 DampedShiftedCoulomb.compute
  *   acs_vv_*                     accusim/integrators.py:25-31 VelocityVerlet.step,
  *                                accusim/system.py:124-129 apply_boundaries, simulation.py:67-70
+ *   acs_rdf_hist                 accusim/analysis.py:7-24 rdf (pair-distance histogram)
  *   acs_langevin_ou              accusim/integrators.py:50-71 Langevin.step (the O-step; B and A reuse acs_vv_*)
  *   acs_reduce_conserved         accusim/system.py:106-114 kinetic_energy / momentum / angular_momentum
  *   acs_engine_*                 accusim/simulation.py:95-112 Simulation.run driving VelocityVerlet with
@@ -89,6 +90,15 @@ int acs_nlist_build(const double* pos, int64_t n, const acs_grid* g, int32_t max
  * Capacity `cap`; pairs beyond it are counted but not written. */
 int acs_nlist_pairs(const int32_t* nbr, const int32_t* nnb, int64_t n, int32_t maxnb, int32_t* pi, int32_t* pj,
                     int64_t cap, unsigned long long* count_dev, void* stream);
+/* Pair-distance histogram for the radial distribution function, replaces the O(n^2) pair loop of
+ * accusim/analysis.py:7-24 (rdf): counts of pairs i < j (both of species `species`; all atoms when it is
+ * negative) with minimum-image distance r <= rmax in `bins` equal bins of [0, rmax], r and the bin index
+ * computed as the reference computes them (FP64 minimum image, sqrt, NumPy's uniform-bin histogram rule).
+ * hist_dev: bins uint64 counts (device). g: a periodic grid from acs_grid_setup with rc >= rmax (the
+ * caller normalises by the ideal-gas shell counts). bins <= 8192. Work from acs_rdf_work_bytes. */
+size_t acs_rdf_work_bytes(int64_t n, const acs_grid* g);
+int acs_rdf_hist(const double* pos, const int32_t* sp, int64_t n, const acs_grid* g, int32_t species, int32_t bins,
+                 double rmax, unsigned long long* hist_dev, void* work, size_t work_bytes, void* stream);
 /* Skin test of accusim/forces.py:88-94: flag_dev = 1 if max_i |x_i - x0_i|^2 (minimum image) >= half_skin2. */
 int acs_nlist_displacement(const double* pos, const double* pos0, int64_t n, const double* box3, int periodic,
                            double half_skin2, int32_t* flag_dev, void* stream);

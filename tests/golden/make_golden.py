@@ -14,6 +14,8 @@ Each case restates a reference test or example setup (file:line inside the accus
   nacl4096                examples/molten_salt.py:22-33 geometry at the 4096-ion / 1.55 g/cm^3 config
   ewald_melt512           tests/test_dsf.py:46-52       Ewald label oracle on a disordered melt
   thermostats108          tests/test_nose_hoover.py:6-17 argon; Langevin BAOAB and Nose-Hoover runs
+  analysis_melt1000       accusim/analysis.py:7-24 rdf (all ions, Na only) on a perturbed rock-salt box
+  analysis_msd108         accusim/analysis.py:27-43 msd, and io_traj108.npz written by accusim/io.py:13-26
 """
 from __future__ import annotations
 
@@ -233,6 +235,38 @@ def thermostats108():
          T=120.0, friction=5e12, seed=11, tau=Q(0.2, "ps").value)
 
 
+def analysis_cases():
+    from accusim import analysis
+    from accusim import io as aio
+    # rdf: 1000 ions of rock salt (10^3 sites, a/2 = 2.82 A) displaced by seeded 0.3 A noise
+    s = System(3, box=10 * 2.82e-10, periodic=True)
+    s.add_species("Na", Q(22.98977, "u").value, charge=1.602176634e-19)
+    s.add_species("Cl", Q(35.453, "u").value, charge=-1.602176634e-19)
+    g = np.stack(np.meshgrid(*[np.arange(10)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    odd = g.sum(1) % 2 == 1
+    rng = np.random.default_rng(17)
+    s.add("Na", ((g[~odd] + 0.5) * 2.82e-10 + rng.normal(0, 0.3e-10, (int((~odd).sum()), 3))) % s.box)
+    s.add("Cl", ((g[odd] + 0.5) * 2.82e-10 + rng.normal(0, 0.3e-10, (int(odd.sum()), 3))) % s.box)
+    rmax = 0.45 * 10 * 2.82e-10
+    r_all, g_all = analysis.rdf(s, rmax, bins=120)
+    r_na, g_na = analysis.rdf(s, rmax, bins=60, species="Na")
+    save("analysis_melt1000", **state_arrays(s), rmax=rmax, r_all=r_all, g_all=g_all, r_na=r_na, g_na=g_na)
+    # msd and io: 108 argon atoms, positions recorded every step for 20 steps of 10 fs
+    m = Q(39.948, "u").value
+    L = (4 * 27 * m / 1374.0) ** (1 / 3)
+    s = System(3, box=L, periodic=True)
+    s.add_species("Ar", m)
+    s.add("Ar", fcc(3, L))
+    s.maxwell_boltzmann(300.0, np.random.default_rng(8))
+    sim = Simulation(s, [LennardJones({"Ar": (120 * k_B.value, 3.4e-10)}, cutoff=2.5)], integrator=VelocityVerlet(),
+                     dt=Q(10, "fs"))
+    tr = sim.run(steps=20, record_every=1, positions=True)
+    t, msd = analysis.msd(tr, box=s.box)
+    save("analysis_msd108", t_frames=np.array(tr.t), frames=np.array(tr.positions), box=s.box.copy(), t=t, msd=msd)
+    aio.save(tr, s, os.path.join(OUT, "io_traj108.npz"))
+    print(f"io_traj108: {os.path.getsize(os.path.join(OUT, 'io_traj108.npz')) / 1024:.0f} KiB")
+
+
 if __name__ == "__main__":
     print("reference accusim", accusim.__version__, "from", os.path.dirname(accusim.__file__))
     lj_mix(True)
@@ -243,3 +277,4 @@ if __name__ == "__main__":
     nacl4096()
     ewald_melt()
     thermostats108()
+    analysis_cases()

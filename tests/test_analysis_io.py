@@ -1,0 +1,39 @@
+"""Trajectory files and the msd observable against files and values written by the reference itself
+(tests/golden/make_golden.py: io_traj108.npz is accusim/io.py:save's own output). CPU only."""
+import os
+
+import numpy as np
+
+from devinproj_b200 import io as bio
+from devinproj_b200.analysis import msd
+from devinproj_b200.system import System
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _system_from_meta(meta, box):
+    s = System(3, box=box, periodic=True)
+    for m in meta:
+        s.add_species(m["name"], m["mass"], charge=m["charge"])
+    return s
+
+
+def test_reference_file_loads_and_saves_back_identically(tmp_path, golden):
+    g = golden("analysis_msd108")
+    tr, meta = bio.load(os.path.join(GOLDEN, "io_traj108.npz"))
+    assert [m["name"] for m in meta] == ["Ar"]
+    assert np.array_equal(np.array(tr.t), g["t_frames"])
+    assert np.array_equal(np.array(tr.positions), g["frames"])
+    out = tmp_path / "again.npz"
+    bio.save(tr, _system_from_meta(meta, g["box"]), out)
+    a, b = np.load(os.path.join(GOLDEN, "io_traj108.npz")), np.load(out)
+    assert sorted(a.files) == sorted(b.files)
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_msd_matches_reference(golden):
+    g = golden("analysis_msd108")
+    tr, _ = bio.load(os.path.join(GOLDEN, "io_traj108.npz"))
+    t, m = msd(tr, box=g["box"])
+    assert np.array_equal(t, g["t"]) and np.array_equal(m, g["msd"])
