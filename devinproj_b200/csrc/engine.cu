@@ -54,6 +54,7 @@ struct RepDev {
   float pad0;
   double dt, hdt, hs2, rl2;
   double lv_c1, lv_pad;                 // Langevin: exp(-gamma dt)
+  double nh_Q, nh_nfkT;                 // Nose-Hoover: thermostat mass, N_f kT
   double lv_sig[ACS_MAX_SPECIES];       // Langevin: sqrt((1 - c1^2) kT / m) per species
 };
 
@@ -95,7 +96,12 @@ struct Eng {
   unsigned int* bar;  // [0] counter, [1] generation
   unsigned long long* phase_ns;  // rebuild phase durations, accumulated (block 0 timestamps)
   const float* fext;             // optional per-slot force added to the pair forces (learned correction)
-  int32_t thermo;                // 0 VelocityVerlet, 1 Langevin BAOAB
+  int32_t thermo;                // 0 VelocityVerlet, 1 Langevin BAOAB, 2 Nose-Hoover
+  double* nh_part;               // Nose-Hoover: per atom group sum m v^2
+  double* nh_chunk;              // Nose-Hoover: per record chunk sum
+  double* nh_st;                 // Nose-Hoover per replica: xi, eta, K2 for the next start half, scale to
+                                 // apply, end-half scale (records), 3 spare (8 doubles)
+  double* rec_bath;              // bath energy per record and replica
   uint32_t seed_lo, seed_hi;
   unsigned long long* octr;      // O-steps taken so far (Langevin draws: counter)
 };
@@ -309,7 +315,10 @@ __device__ __forceinline__ void drift_or_baoab(const Eng& E, const RepDev& R, in
   }
 }
 
-template <bool LJ, bool DSF, bool REC, int MODE, bool ONE, bool LV = false>
+// TH: 0 VelocityVerlet, 1 Langevin BAOAB (the drift of MODE 0 becomes A-O-A), 2 Nose-Hoover (MODE 0 stops
+// after the second kick like MODE 1: the thermostat's global kinetic-energy sum comes first; every mode
+// writes the group's sum of m v^2 to nh_part).
+template <bool LJ, bool DSF, bool REC, int MODE, bool ONE, int TH = 0>
 __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int dst, unsigned ostep) {
   __shared__ float4 shift_tab[8][27];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -342,6 +351,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
     }
     const bool valid = (i - R.atom0) < R.n;
     double rv[kRecW] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double k2 = 0.0;
     double dfx = 0.0, dfy = 0.0, dfz = 0.0, deu = 0.0;
     float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
     int si = 0;
@@ -429,12 +439,13 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         rv[6] = z * px - x * pz;
         rv[7] = x * py - y * px;
       }
-      if (MODE == 0) {
+      if (TH == 2) k2 = ff.mass[si] * (vx * vx + vy * vy + vz * vz);
+      if (MODE == 0 && TH != 2) {
         vx += R.hdt * ax;
         vy += R.hdt * ay;
         vz += R.hdt * az;
         double ux, uy, uz;
-        drift_or_baoab<LV>(E, R, i, r, si, ostep, vx, vy, vz, ux, uy, uz);
+        drift_or_baoab<TH == 1>(E, R, i, r, si, ostep, vx, vy, vz, ux, uy, uz);
         E.u[3 * i] = ux;
         E.u[3 * i + 1] = uy;
         E.u[3 * i + 2] = uz;
@@ -461,6 +472,118 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         if (lane == 0) E.partials[(int64_t)w * kRecW + q] = x;
       }
     }
+    if (TH == 2) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) k2 += __shfl_down_sync(0xffffffffu, k2, o);
+      if (lane == 0) E.nh_part[w] = k2;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------- Nose-Hoover --
+// Per record chunk: the groups' sums of m v^2 in group order (deterministic).
+__global__ void k_nh_chunks(Eng E) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < E.nchunks_total; c += gridDim.x * blockDim.x) {
+    if (!E.active[E.chunk_rep[c]]) continue;
+    double s = 0.0;
+    const int t0 = E.chunk_tile0[c], nt = E.chunk_ntiles[c];
+    for (int t = 0; t < nt; ++t) s += E.nh_part[t0 + t];
+    E.nh_chunk[c] = s;
+  }
+}
+
+// Thermostat scalars, one thread per replica, with the half-step of accusim/integrators.py:94-103:
+//   xi += dt/4 (K2 - N_f kT) / Q;  s = exp(-dt/2 xi);  eta += dt/2 xi;  xi += dt/4 (K2 s^2 - N_f kT) / Q
+// (K2 = sum m v^2, the velocities then scale by s). mode 0: initial state (K2 kept for the first start
+// half); 1: start half of a block's first step; 2: end half of a block's last step; 3: end half of step k
+// then start half of step k + 1 (K2 s1^2 is the scaled velocities' sum). Writes the scale to apply, the
+// end-half scale for the records and, on record steps, the bath energy Q xi^2 / 2 + N_f kT eta.
+__global__ void k_nh_scalars(Eng E, int mode, int rec, int rec_idx) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= E.R || !E.active[r]) return;
+  const RepDev& R = E.rep[r];
+  double* st = E.nh_st + 8 * (int64_t)r;
+  double xi = st[0], eta = st[1];
+  const double dt = R.dt, Q = R.nh_Q, nfkT = R.nh_nfkT;
+  auto half = [&](double k2) {
+    xi += 0.25 * dt * (k2 - nfkT) / Q;
+    const double sc = exp(-0.5 * dt * xi);
+    eta += 0.5 * dt * xi;
+    xi += 0.25 * dt * (k2 * (sc * sc) - nfkT) / Q;
+    return sc;
+  };
+  double k2 = 0.0;
+  if (mode != 1) {
+    for (int c = 0; c < R.nchunks; ++c) k2 += E.nh_chunk[R.chunk0 + c];
+  }
+  // records hold the state after the step's end half (accusim/simulation.py:88 records after the step)
+  auto record = [&]() {
+    if (rec && rec_idx < E.rec_cap) E.rec_bath[(int64_t)rec_idx * E.R + r] = 0.5 * Q * (xi * xi) + nfkT * eta;
+  };
+  if (mode == 0) {
+    st[2] = k2;
+    st[3] = 1.0;
+    st[4] = 1.0;
+    record();
+  } else if (mode == 1) {
+    st[3] = half(st[2]);
+  } else {
+    const double s1 = half(k2);
+    const double k2e = k2 * (s1 * s1);
+    st[4] = s1;
+    record();
+    if (mode == 3) {
+      st[3] = s1 * half(k2e);
+    } else {
+      st[3] = s1;
+      st[2] = k2e;
+    }
+  }
+  st[0] = xi;
+  st[1] = eta;
+}
+
+// Sum of m v^2 per atom group (groups of G slots, the step kernel's grouping) from the stored velocities.
+__global__ void k_nh_ke(Eng E, FFDev ff) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < E.NG; w += gridDim.x * blockDim.x) {
+    double k2 = 0.0;
+    for (int q = 0; q < E.G; ++q) {
+      const int64_t i = (int64_t)w * E.G + q;
+      const int r = E.tile_rep[i >> 5];
+      if (!E.active[r] || i - E.rep[r].atom0 >= E.rep[r].n) continue;
+      const double vx = E.v[3 * i], vy = E.v[3 * i + 1], vz = E.v[3 * i + 2];
+      k2 += ff.mass[E.sp[i]] * (vx * vx + vy * vy + vz * vz);
+    }
+    E.nh_part[w] = k2;
+  }
+}
+
+// Apply the thermostat scale per atom; `full`: then the first kick, drift, image and skin test of the next
+// step (what k_step's MODE 0 does without a thermostat).
+__global__ void k_nh_apply(Eng E, int full, int dst) {
+  if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E.S; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[i >> 5];
+    if (!E.active[r]) continue;
+    const RepDev& R = E.rep[r];
+    if (i - R.atom0 >= R.n) continue;
+    const double sc = E.nh_st[8 * (int64_t)r + 3];
+    double vx = sc * E.v[3 * i], vy = sc * E.v[3 * i + 1], vz = sc * E.v[3 * i + 2];
+    if (full) {
+      vx += R.hdt * E.acc[3 * i];
+      vy += R.hdt * E.acc[3 * i + 1];
+      vz += R.hdt * E.acc[3 * i + 2];
+      const double ux = E.u[3 * i] + R.dt * vx, uy = E.u[3 * i + 1] + R.dt * vy, uz = E.u[3 * i + 2] + R.dt * vz;
+      E.u[3 * i] = ux;
+      E.u[3 * i + 1] = uy;
+      E.u[3 * i + 2] = uz;
+      E.img[dst][i] = make_img(ux, uy, uz, E.sp[i]);
+      const double ddx = ux - E.u0[3 * i], ddy = uy - E.u0[3 * i + 1], ddz = uz - E.u0[3 * i + 2];
+      if (!(ddx * ddx + ddy * ddy + ddz * ddz < R.hs2)) E.flag[r] = 1;
+    }
+    E.v[3 * i] = vx;
+    E.v[3 * i + 1] = vy;
+    E.v[3 * i + 2] = vz;
   }
 }
 
@@ -475,9 +598,10 @@ __global__ void k_prologue(Eng E, int dst) {
     if (!E.active[r]) continue;
     const RepDev& R = E.rep[r];
     if (i - R.atom0 >= R.n) continue;
-    double vx = E.v[3 * i] + R.hdt * E.acc[3 * i];
-    double vy = E.v[3 * i + 1] + R.hdt * E.acc[3 * i + 1];
-    double vz = E.v[3 * i + 2] + R.hdt * E.acc[3 * i + 2];
+    const double sc = E.thermo == 2 ? E.nh_st[8 * (int64_t)r + 3] : 1.0;   // Nose-Hoover start half
+    double vx = sc * E.v[3 * i] + R.hdt * E.acc[3 * i];
+    double vy = sc * E.v[3 * i + 1] + R.hdt * E.acc[3 * i + 1];
+    double vz = sc * E.v[3 * i + 2] + R.hdt * E.acc[3 * i + 2];
     double ux, uy, uz;
     if (E.thermo == 1) drift_or_baoab<true>(E, R, i, r, E.sp[i], 0u, vx, vy, vz, ux, uy, uz);
     else drift_or_baoab<false>(E, R, i, r, E.sp[i], 0u, vx, vy, vz, ux, uy, uz);
@@ -675,6 +799,10 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       const RepDev& R = E.rep[r];
       double s = 0.0;
       for (int c = 0; c < R.nchunks; ++c) s += E.chunk_part[(int64_t)(R.chunk0 + c) * kRecW + threadIdx.x];
+      if (E.thermo == 2) {  // the partials predate the step's end half: KE scales by s^2, P and L by s
+        const double s1 = E.nh_st[8 * (int64_t)r + 4];
+        s *= threadIdx.x == 0 ? s1 * s1 : (threadIdx.x == 1 ? 1.0 : s1);
+      }
       if (rec_idx < E.rec_cap) E.rec[((int64_t)rec_idx * E.R + r) * kRecW + threadIdx.x] = s;
     }
   }
@@ -1349,8 +1477,9 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
   }
   const int G = 32 / tpa;
   err = ACS_OK;
-  if (cfg->thermo.kind < 0 || cfg->thermo.kind > 1 ||
-      (cfg->thermo.kind == 1 && !(cfg->thermo.kT >= 0.0 && cfg->thermo.friction >= 0.0))) {
+  if (cfg->thermo.kind < 0 || cfg->thermo.kind > 2 ||
+      (cfg->thermo.kind == 1 && !(cfg->thermo.kT >= 0.0 && cfg->thermo.friction >= 0.0)) ||
+      (cfg->thermo.kind == 2 && !(cfg->thermo.kT > 0.0 && cfg->thermo.period > 0.0))) {
     err = ACS_ERR_ARG;
     return;
   }
@@ -1404,6 +1533,11 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     R.hdt = 0.5 * q.dt;
     R.hs2 = q.half_skin * q.half_skin;
     R.rl2 = q.rlist * q.rlist;
+    if (cfg->thermo.kind == 2) {  // accusim/integrators.py:86-92: N_f = dim (n - 1), Q = N_f kT tau^2
+      const double nf = 3.0 * (double)std::max(q.n - 1, 1);
+      R.nh_nfkT = nf * cfg->thermo.kT;
+      R.nh_Q = nf * cfg->thermo.kT * (cfg->thermo.period * cfg->thermo.period);
+    }
     if (cfg->thermo.kind == 1) {  // accusim/integrators.py:65-66
       R.lv_c1 = exp(-cfg->thermo.friction * q.dt);
       for (int t = 0; t < cfg->ff.n_species && t < ACS_MAX_SPECIES; ++t)
@@ -1469,6 +1603,10 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(8 * 16);                             // 40 phase timers
   L.add(4 * (size_t)S);                      // 41 perm2
   L.add(8);                                  // 42 Langevin O-step counter
+  L.add(8 * (size_t)NG);                     // 43 Nose-Hoover group partials
+  L.add(8 * (size_t)NCH);                    // 44 Nose-Hoover chunk partials
+  L.add(8 * 8 * (size_t)R);                  // 45 Nose-Hoover state
+  L.add(8 * (size_t)rec_cap * R);            // 46 bath-energy records
   return L;
 }
 
@@ -1520,18 +1658,40 @@ FFDev make_ff(const acs_forcefield& f, int& err) {
 template <bool LJ, bool DSF, bool ONE>
 int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, unsigned ostep, cudaStream_t s) {
   dim3 g(e->step_blocks), b(e->step_threads);
-  if (mode == 0 && e->E.thermo == 1) {
-    if (rec) k_step<LJ, DSF, true, 0, ONE, true><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
-    else k_step<LJ, DSF, false, 0, ONE, true><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
-  } else if (mode == 0) {
-    if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
-    else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+  const int th = e->E.thermo;
+  if (mode == 0) {
+    if (th == 1) {
+      if (rec) k_step<LJ, DSF, true, 0, ONE, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else k_step<LJ, DSF, false, 0, ONE, 1><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    } else if (th == 2) {
+      if (rec) k_step<LJ, DSF, true, 0, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else k_step<LJ, DSF, false, 0, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    } else {
+      if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    }
   } else if (mode == 1) {
-    if (rec) k_step<LJ, DSF, true, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
-    else k_step<LJ, DSF, false, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    if (th == 2) {
+      if (rec) k_step<LJ, DSF, true, 1, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else k_step<LJ, DSF, false, 1, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    } else {
+      if (rec) k_step<LJ, DSF, true, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else k_step<LJ, DSF, false, 1, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    }
   } else {
-    k_step<LJ, DSF, true, 2, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    if (th == 2) k_step<LJ, DSF, true, 2, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+    else k_step<LJ, DSF, true, 2, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
   }
+  return launch_status();
+}
+
+// Nose-Hoover after a step kernel (or at set-up): chunk sums of m v^2, the thermostat scalars (mode as in
+// k_nh_scalars) and, after a step (modes 2, 3), the per-atom scale, for mode 3 with the next kick and drift.
+int launch_nh(acs_engine* e, int mode, int rec, int rec_idx, int dst, cudaStream_t s) {
+  if (e->E.thermo != 2) return ACS_OK;
+  if (mode != 1) k_nh_chunks<<<(e->E.nchunks_total + 255) / 256, 256, 0, s>>>(e->E);
+  k_nh_scalars<<<(e->E.R + 63) / 64, 64, 0, s>>>(e->E, mode, rec, rec_idx);
+  if (mode == 2 || mode == 3) k_nh_apply<<<e->step_blocks, 256, 0, s>>>(e->E, mode == 3 ? 1 : 0, dst);
   return launch_status();
 }
 
@@ -1578,6 +1738,7 @@ int launch_rebuild(acs_engine* e, int dst, int rec, int rec_idx, int force_all, 
 // accelerations. Image buffers alternate 0,1.
 int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cudaStream_t s) {
   int st = ACS_OK;
+  if ((st = launch_nh(e, 1, 0, 0, 0, s))) return st;   // Nose-Hoover start half of the block's first step
   k_prologue<<<e->step_blocks, 256, 0, s>>>(e->E, 0);
   if ((st = launch_status())) return st;
   if ((st = launch_rebuild(e, 0, 0, 0, 0, s))) return st;
@@ -1588,6 +1749,7 @@ int enqueue_block(acs_engine* e, int steps, const std::vector<char>& rec_at, cud
     const int rec = rec_at[k] ? 1 : 0;
     if (k % e->c_stride == 0 && (st = launch_correction(e, src, s))) return st;
     if ((st = launch_step(e, rec, last ? 1 : 0, src, dst, (unsigned)(k + 1), s))) return st;
+    if ((st = launch_nh(e, last ? 2 : 3, rec, rec_idx, dst, s))) return st;
     if (!last || rec) {
       if ((st = launch_rebuild(e, dst, rec, rec_idx, 0, s))) return st;
     }
@@ -1700,6 +1862,10 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.phase_ns = (unsigned long long*)(b + L.off[40]);
   E.perm2 = (int32_t*)(b + L.off[41]);
   E.octr = (unsigned long long*)(b + L.off[42]);
+  E.nh_part = (double*)(b + L.off[43]);
+  E.nh_chunk = (double*)(b + L.off[44]);
+  E.nh_st = (double*)(b + L.off[45]);
+  E.rec_bath = (double*)(b + L.off[46]);
   E.thermo = cfg->thermo.kind;
   E.seed_lo = (uint32_t)cfg->thermo.seed;
   E.seed_hi = (uint32_t)(cfg->thermo.seed >> 32);
@@ -1745,6 +1911,8 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   ok = ok && cudaMemset(E.nnb, 0, 4 * (size_t)S) == cudaSuccess;
   ok = ok && cudaMemset(E.phase_ns, 0, 8 * 16) == cudaSuccess;
   ok = ok && cudaMemset(E.octr, 0, 8) == cudaSuccess;
+  ok = ok && cudaMemset(E.nh_st, 0, 8 * 8 * (size_t)E.R) == cudaSuccess;
+  ok = ok && cudaMemset(E.rec_bath, 0, 8 * (size_t)E.rec_cap * E.R) == cudaSuccess;
   int sms = 0, per_sm = 0;
   ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev) == cudaSuccess;
   ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, 256, 0) == cudaSuccess;
@@ -1771,6 +1939,7 @@ int acs_engine_set_state(acs_engine* e, const double* pos, const double* vel, co
   if ((st = launch_rebuild(e, 0, 0, 0, 1, s))) return st;
   if ((st = launch_correction(e, 0, s))) return st;
   if ((st = launch_step(e, 1, 2, 0, 0, 0u, s))) return st;
+  if ((st = launch_nh(e, 0, 1, 0, 0, s))) return st;
   return launch_rebuild(e, 0, 1, 0, 0, s);
 }
 
@@ -1881,7 +2050,11 @@ int acs_engine_launch_info(acs_engine* e, int32_t* step_blocks, int32_t* coop_bl
 int acs_engine_load_state(acs_engine* e, const double* pos, const double* vel, void* stream) {
   if (!e || !pos || !vel) return ACS_ERR_ARG;
   k_load_keep<<<e->step_blocks, 256, 0, (cudaStream_t)stream>>>(e->E, pos, vel, e->src0_dev);
-  return launch_status();
+  int st = launch_status();
+  if (st || e->E.thermo != 2) return st;
+  // new velocities: the next start half needs their kinetic-energy sum
+  k_nh_ke<<<(e->E.NG + 255) / 256, 256, 0, (cudaStream_t)stream>>>(e->E, e->ff);
+  return launch_nh(e, 0, 0, 0, 0, (cudaStream_t)stream);
 }
 
 int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* stream) {
@@ -1913,8 +2086,9 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
     ne += 2;
     return r;
   };
-  k_prologue<<<e->step_blocks, 256, 0, s>>>(e->E, 0);
-  st = launch_status();
+  st = launch_nh(e, 1, 0, 0, 0, s);
+  if (!st) k_prologue<<<e->step_blocks, 256, 0, s>>>(e->E, 0);
+  if (!st) st = launch_status();
   if (!st) st = launch_rebuild(e, 0, 0, 0, 0, s);
   int rec_idx = 0;
   for (int k = 0; k < steps && !st; ++k) {
@@ -1922,7 +2096,10 @@ int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, flo
     const bool last = (k == steps - 1);
     const int rec = ((record_every > 0 && (k + 1) % record_every == 0) || last) ? 1 : 0;
     if (e->corr && k % e->c_stride == 0) st = mark(2, [&] { return launch_correction(e, src, s); });
-    if (!st) st = mark(0, [&] { return launch_step(e, rec, last ? 1 : 0, src, dst, (unsigned)(k + 1), s); });
+    if (!st) st = mark(0, [&] {
+      int q = launch_step(e, rec, last ? 1 : 0, src, dst, (unsigned)(k + 1), s);
+      return q ? q : launch_nh(e, last ? 2 : 3, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, dst, s);
+    });
     if (!st) st = mark(1, [&] { return launch_rebuild(e, dst, rec, rec_idx < e->E.rec_cap ? rec_idx : 0, 0, s); });
     rec_idx += rec;
   }
@@ -1986,6 +2163,30 @@ int acs_engine_set_correction(acs_engine* e, const float* params6, const float* 
 }
 
 float acs_engine_last_correction_ms(acs_engine* e) { return e ? e->last_corr_ms : 0.f; }
+
+int acs_engine_nh_state(acs_engine* e, double* xi_eta, int32_t set) {
+  if (!e || !xi_eta) return ACS_ERR_ARG;
+  std::vector<double> st(8 * (size_t)e->E.R);
+  if (cudaMemcpy(st.data(), e->E.nh_st, 8 * st.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return ACS_ERR_CUDA;
+  for (int r = 0; r < e->E.R; ++r) {
+    if (set) {
+      st[8 * r] = xi_eta[2 * r];
+      st[8 * r + 1] = xi_eta[2 * r + 1];
+    } else {
+      xi_eta[2 * r] = st[8 * r];
+      xi_eta[2 * r + 1] = st[8 * r + 1];
+    }
+  }
+  if (set && cudaMemcpy(e->E.nh_st, st.data(), 8 * st.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return ACS_ERR_CUDA;
+  return ACS_OK;
+}
+
+int acs_engine_bath_records(acs_engine* e, double* out_dev, int32_t count, void* stream) {
+  if (!e || !out_dev || count < 0 || count > e->E.rec_cap) return ACS_ERR_ARG;
+  return cudaMemcpyAsync(out_dev, e->E.rec_bath, 8 * (size_t)count * e->E.R, cudaMemcpyDeviceToDevice,
+                         (cudaStream_t)stream) == cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
+}
 
 int acs_engine_set_correction_stride(acs_engine* e, int32_t stride) {
   if (!e || stride < 1) return ACS_ERR_ARG;

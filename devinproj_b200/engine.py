@@ -47,7 +47,7 @@ class ForceField(C.Structure):
 
 class Thermostat(C.Structure):
     _fields_ = [("kind", C.c_int32), ("pad", C.c_int32), ("kT", C.c_double), ("friction", C.c_double),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("period", C.c_double)]
 
 
 class EngineConfig(C.Structure):
@@ -61,7 +61,14 @@ def langevin_thermostat(integrator, seed):
     friction) in engine units; seed None draws one."""
     if seed is None:
         seed = int(np.random.default_rng().integers(2 ** 63))
-    return Thermostat(1, 0, k_B * float(integrator.T) / ENERGY, float(integrator.gamma) * TIME, int(seed) % 2 ** 64)
+    return Thermostat(1, 0, k_B * float(integrator.T) / ENERGY, float(integrator.gamma) * TIME, int(seed) % 2 ** 64,
+                      0.0)
+
+
+def nose_hoover_thermostat(integrator):
+    """Engine thermostat block for a Nose-Hoover integrator (this package's or the reference's: SI T and
+    period) in engine units."""
+    return Thermostat(2, 0, k_B * float(integrator.T) / ENERGY, 0.0, 0, float(integrator.tau) / TIME)
 
 
 class DevStatusC(C.Structure):
@@ -86,6 +93,8 @@ ENGINE_SIGNATURES = {
     "acs_engine_phase_times": (C.c_int, [P, P, C.c_int]),
     "acs_engine_set_correction": (C.c_int, [P, P, P, P, P, P, P, C.c_float, P, P, P, P, C.c_int]),
     "acs_engine_last_correction_ms": (C.c_float, [P]),
+    "acs_engine_nh_state": (C.c_int, [P, P, C.c_int32]),
+    "acs_engine_bath_records": (C.c_int, [P, P, C.c_int32, P]),
     "acs_engine_set_correction_stride": (C.c_int, [P, C.c_int32]),
     "acs_engine_destroy": (C.c_int, [P]),
 }
@@ -277,6 +286,25 @@ class Engine:
                    "acs_engine_records")
         return self._rec_buf[: count * self.R * 8].view(count, self.R, 8).cpu().numpy()
 
+    def bath_records(self, count: int) -> np.ndarray:
+        """(count, R) thermostat energies at the records (Nose-Hoover; zero otherwise), engine units."""
+        if count == 0:
+            return np.zeros((0, self.R))
+        buf = torch.empty(count * self.R, dtype=torch.float64, device="cuda")
+        _lib.check(self.L.acs_engine_bath_records(self.h, buf.data_ptr(), int(count), stream_handle()),
+                   "acs_engine_bath_records")
+        return buf.view(count, self.R).cpu().numpy()
+
+    def nh_state(self) -> np.ndarray:
+        """(R, 2) Nose-Hoover (xi, eta) per replica, engine units."""
+        out = np.zeros((self.R, 2))
+        _lib.check(self.L.acs_engine_nh_state(self.h, out.ctypes.data, 0), "acs_engine_nh_state")
+        return out
+
+    def set_nh_state(self, xi_eta):
+        arr = np.ascontiguousarray(np.asarray(xi_eta, dtype=np.float64).reshape(self.R, 2))
+        _lib.check(self.L.acs_engine_nh_state(self.h, arr.ctypes.data, 1), "acs_engine_nh_state")
+
     def status(self, clear=False) -> DevStatusC:
         st = DevStatusC()
         _lib.check(self.L.acs_engine_status(self.h, C.byref(st), 1 if clear else 0, stream_handle()),
@@ -378,8 +406,9 @@ class GpuSimulation:
     """`Simulation` with the step loop on the device (accusim/simulation.py:40-131 interface).
 
     forces: [LennardJones] and/or [DampedShiftedCoulomb] (this package's or the reference's classes);
-    integrator: VelocityVerlet, or Langevin (BAOAB, counter-based draws keyed by `seed`). `system.pos`/`vel`
-    are synchronised from the device after every `run` call (and at records when positions=True)."""
+    integrator: VelocityVerlet, Langevin (BAOAB, counter-based draws keyed by `seed`) or NoseHoover (its xi,
+    eta and Q kept in the integrator object, bath energy in the trajectory). `system.pos`/`vel` are
+    synchronised from the device after every `run` call (and at records when positions=True)."""
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
                  rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500, correction_stride=1):
@@ -389,9 +418,11 @@ class GpuSimulation:
         if reactions:
             raise NotImplementedError("reactions are not part of the accusim_b200 force-and-step path")
         kind = type(integrator).__name__ if integrator is not None else "VelocityVerlet"
-        if kind not in ("VelocityVerlet", "Langevin"):
-            raise ValueError("GpuSimulation integrates with VelocityVerlet or Langevin (BAOAB)")
-        thermo = langevin_thermostat(integrator, seed) if kind == "Langevin" else None
+        if kind not in ("VelocityVerlet", "Langevin", "NoseHoover"):
+            raise ValueError("GpuSimulation integrates with VelocityVerlet, Langevin (BAOAB) or NoseHoover")
+        thermo = (langevin_thermostat(integrator, seed) if kind == "Langevin"
+                  else nose_hoover_thermostat(integrator) if kind == "NoseHoover" else None)
+        self._nh = kind == "NoseHoover"
         self.system = system
         self.forces = list(forces)
         self.integrator = integrator or VelocityVerlet()
@@ -406,14 +437,33 @@ class GpuSimulation:
         self.engine, self.rlist, self.half_skin = start_engine(
             [system], self.forces, [self.dt if self.dt is not None else 1e-15], maxnb=maxnb, rec_cap=rec_cap,
             grid_mult=grid_mult, tpa=tpa, thermo=thermo)
+        if self._nh:   # continue the integrator's thermostat state; the initial record then carries its energy
+            self.engine.set_nh_state([[float(self.integrator.xi) * TIME, float(self.integrator.eta)]])
+            _upload_state(self.engine, [system])
+            self.engine.check("thermostat state")
         self.correction = None
         self.validate_every = int(validate_every)
         self.validations = []
         self.engine.set_correction_stride(correction_stride)
         if correction is not None:
             self.set_correction(correction)
-        self._last = self.engine.records(1)[0, 0]
+        self._last, self._last_bath = self._latest()
         self._pull()
+
+    def _latest(self):
+        """The engine's latest record and bath energy (engine units)."""
+        return self.engine.records(1)[0, 0], (self.engine.bath_records(1)[0, 0] if self._nh else 0.0)
+
+    def _sync_thermostat(self):
+        """Nose-Hoover: the integrator object holds the run's (xi, eta) and Q, as the reference's does."""
+        if not self._nh:
+            return
+        xi, eta = self.engine.nh_state()[0]
+        it = self.integrator
+        it.xi, it.eta = float(xi) / TIME, float(eta)
+        if it.Q is None:
+            nf = it.dof(self.system)
+            it.Q = nf * (k_B * it.T) * it.tau ** 2
 
     def set_correction(self, lc, enabled=True):
         """Add a trained LearnedCorrection to the DSF forces (re-evaluates the current forces)."""
@@ -421,7 +471,7 @@ class GpuSimulation:
         self.correction = lc if enabled else None
         _upload_state(self.engine, [self.system])
         self.engine.check("set_correction")
-        self._last = self.engine.records(1)[0, 0]
+        self._last, self._last_bath = self._latest()
         self._pull()
 
     def validate(self):
@@ -451,7 +501,7 @@ class GpuSimulation:
     def rebuilds(self):
         return int(self.engine.status().rebuilds)
 
-    def _record(self, rec, positions):
+    def _record(self, rec, positions, bath=0.0):
         s, tr = self.system, self.trajectory
         tr.t.append(self.time)
         tr.kinetic.append(float(rec[0] * ENERGY))
@@ -463,7 +513,7 @@ class GpuSimulation:
         tr.mass.append(float(np.sum(s.masses)))
         tr.charge.append(float(np.sum(s.charges)))
         tr.counts.append(s.counts())
-        tr.bath.append(0.0)
+        tr.bath.append(float(bath * ENERGY))
         if positions:
             tr.positions.append(s.pos.copy())
             tr.velocities.append(s.vel.copy())
@@ -482,7 +532,7 @@ class GpuSimulation:
         if not self.trajectory.t:
             if self._initial is None:
                 self._initial = _InitialState(self.system.copy(), self)
-            self._record(self._last, positions)
+            self._record(self._last, positions, self._last_bath)
         eng = self.engine
         done = 0
         while done < steps:
@@ -500,25 +550,27 @@ class GpuSimulation:
             if not local or local[-1] != block:
                 local.append(block)
             recs = eng.records(len(local))[:, 0, :]
+            baths = eng.bath_records(len(local))[:, 0] if self._nh else np.zeros(len(local))
             eng.check("engine run")
-            kept = [(j, rec) for j, rec in zip(local, recs) if (done + j) % re == 0 or done + j == steps]
+            kept = [(j, rec, b) for j, rec, b in zip(local, recs, baths) if (done + j) % re == 0 or done + j == steps]
             if positions and kept:
                 self._pull_positions()
             j0 = 0
-            for j, rec in kept:
+            for j, rec, b in kept:
                 for _ in range(j - j0):
                     self.time += self.dt
                 j0 = j
-                self._record(rec, positions)
+                self._record(rec, positions, b)
             for _ in range(block - j0):
                 self.time += self.dt
-            self._last = recs[-1]
+            self._last, self._last_bath = recs[-1], baths[-1]
             self.steps += block
             done += block
             if self.correction is not None and self.validate_every > 0 and self.steps % self.validate_every == 0:
                 self._pull()
                 self.validate()
         self._pull()
+        self._sync_thermostat()
         return self.trajectory
 
     def _pull_positions(self):
@@ -530,7 +582,7 @@ class GpuSimulation:
         """Re-evaluate forces of the current host state on the device (after host-side edits)."""
         _upload_state(self.engine, [self.system])
         self.engine.check("update_forces")
-        self._last = self.engine.records(1)[0, 0]
+        self._last, self._last_bath = self._latest()
         self._pull()
 
     def clone(self, dt=None):

@@ -45,13 +45,16 @@ typedef struct acs_forcefield {
  * Langevin BAOAB (accusim/integrators.py:50-71) with c1 = exp(-friction dt) and sigma = sqrt((1 - c1^2)
  * kT / m) per species and replica. Its standard normal draws are counter-based (Philox4x32-10, key = seed,
  * counter = (O-step index, atom index within the replica, replica)), so a run is reproducible and does
- * not depend on list rebuilds or on which other replicas share the engine. */
+ * not depend on list rebuilds or on which other replicas share the engine. kind 2: Nose-Hoover with the
+ * Trotter half-steps of accusim/integrators.py:74-116, one thermostat per replica (N_f = 3 (n - 1),
+ * Q = N_f kT period^2), its (xi, eta) read and set with acs_engine_nh_state. */
 typedef struct acs_thermostat {
   int32_t kind;
   int32_t pad;
   double kT;          /* k_B T in the caller's energy unit */
-  double friction;    /* gamma, in 1 / caller time unit */
-  uint64_t seed;
+  double friction;    /* Langevin gamma, in 1 / caller time unit */
+  uint64_t seed;      /* Langevin draws */
+  double period;      /* Nose-Hoover thermostat period, caller time unit */
 } acs_thermostat;
 
 typedef struct acs_engine_config {
@@ -112,6 +115,13 @@ int acs_engine_set_correction(acs_engine* e, const float* params6, const float* 
 int acs_engine_set_correction_stride(acs_engine* e, int32_t stride);
 /* Mean duration (ms) of the correction launches in the last acs_engine_run_timed call. */
 float acs_engine_last_correction_ms(acs_engine* e);
+/* Nose-Hoover state per replica, (xi, eta) pairs in caller units (host array of 2 n_replicas): set = 0
+ * reads it into xi_eta, set = 1 writes it from xi_eta (before a run, e.g. from the integrator object).
+ * Synchronous. */
+int acs_engine_nh_state(acs_engine* e, double* xi_eta, int32_t set);
+/* Thermostat (bath) energy Q xi^2 / 2 + N_f kT eta at each record (Nose-Hoover; 0 otherwise): record i of
+ * replica r at out_dev[i * n_replicas + r], device array. */
+int acs_engine_bath_records(acs_engine* e, double* out_dev, int32_t count, void* stream);
 int acs_engine_destroy(acs_engine* e);
 
 #ifdef __cplusplus
