@@ -475,7 +475,7 @@ class GpuSimulation:
         self._pull()
 
     def validate(self):
-        """Judge the corrected electrostatic forces against the device Ewald on the current state; switch the
+        """Check the corrected electrostatic forces against the device Ewald on the current state; switch the
         correction off (fallback to plain DSF) unless it improves on DSF. Returns (err_dsf, err_corrected)."""
         from .ewald import Ewald
         dsf = [f for f in self.forces if type(f).__name__ == "DampedShiftedCoulomb"][0]

@@ -11,7 +11,7 @@ F_Ewald - F_DSF per ion from its local environment and adds it to DSF:
 * prediction: F_i = scale * sum_c C_c(D_i) V_c(i), rotation-equivariant by construction;
 * training: Adam on labels from the device Ewald (parity-checked against the reference's Ewald) minus
   FP64 DSF, on snapshots of a NaCl melt;
-* validation: the corrected forces are judged against Ewald; if they are not better than plain DSF the
+* validation: the corrected forces are checked against Ewald; if they are not better than plain DSF the
   correction is switched off (fallback to plain DSF).
 """
 from __future__ import annotations
@@ -286,7 +286,7 @@ def pair_kernel_bound(data, train_idx, test_idx, R, spacing=0.25e-10, device="cu
 
 
 class LearnedCorrection:
-    """DSF + learned residual: fit on a dataset, predict corrections, judge against Ewald."""
+    """DSF + learned residual: fit on a dataset, predict corrections, check against Ewald."""
 
     def __init__(self, seed=0):
         self.desc = DescriptorBuilder()
@@ -373,7 +373,7 @@ class LearnedCorrection:
         return float(np.mean(e0)), float(np.mean(e1))
 
     def validate(self, s, dsf_force, ewald_force):
-        """Judge the corrected forces on one state against Ewald; switch the correction off (fallback to plain
+        """Check the corrected forces on one state against Ewald; switch the correction off (fallback to plain
         DSF) unless it improves on DSF by more than 0.1 % relative. Returns (err_dsf, err_corrected, enabled)."""
         e0 = rms_rel(dsf_force, ewald_force)
         e1 = rms_rel(dsf_force + self.predict(s), ewald_force)
@@ -398,7 +398,7 @@ if __name__ == "__main__":   # pragma: no cover - manual training run
     ap = argparse.ArgumentParser(description="train the learned DSF->Ewald correction on an 8000-ion NaCl melt")
     ap.add_argument("--snapshots", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=20)
-    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "..", "gpurun_out", "learned_dsf.npz"))
+    ap.add_argument("--out", default="learned_dsf.npz")
     a = ap.parse_args()
     d = generate_dataset(a.snapshots, verbose=True)
     n_train = int(0.9 * a.snapshots)

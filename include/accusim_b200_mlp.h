@@ -4,7 +4,7 @@
  * acs_ewald_fp64 replaces accusim/forces.py:333-388 (Ewald.compute) on the device, FP64: the caller passes
  * the k-vectors and weights exactly as the reference builds them (accusim/forces.py:347-357), so the
  * result follows the reference's real-space, reciprocal and self terms. It labels training data for the
- * learned correction and judges its error.
+ * learned correction and measures its error.
  *
  * The learned correction has no counterpart in the reference: a BF16 tensor-core (tcgen05) MLP on per-ion
  * radial descriptors predicting the Ewald-minus-DSF force residual (see acs_mlp_* below).

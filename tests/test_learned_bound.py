@@ -1,4 +1,4 @@
-"""The pair-kernel error floor used to judge the learned correction (CPU, FP64): on a synthetic residual
+"""The pair-kernel error floor used to assess the learned correction (CPU, FP64): on a synthetic residual
 that is exactly pair-additive within R, the fit recovers it; a residual from beyond R is not recovered."""
 import numpy as np
 
