@@ -63,3 +63,53 @@ def test_grid_setup_open_system_and_bad_args():
     assert list(g.ncell) == [6, 1, 1] and g.periodic == 0 and g.span[2] == 1.5
     assert _lib.lib().acs_grid_setup(C.byref(g), None, 0, None, None, 1.5) == _lib.ACS_ERR_ARG
     assert _lib.lib().acs_grid_setup(C.byref(g), lo.ctypes.data, 1, None, None, 0.0) == _lib.ACS_ERR_ARG
+
+
+def _engine_config(n=864, box_sigma=10.229, tpa=1, maxnb=96, thermo=None):
+    from devinproj_b200 import engine as E
+    reps = (E.Replica * 1)()
+    reps[0].n = n
+    for d in range(3):
+        reps[0].box[d] = box_sigma * 3.4
+    reps[0].dt = 0.02
+    reps[0].rlist = 2.8 * 3.4
+    reps[0].half_skin = 0.15 * 3.4
+    ff = E.ForceField()
+    ff.n_species, ff.lj = 1, 1
+    ff.mass[0] = 39.948
+    ff.lj_eps[0], ff.lj_sig[0], ff.lj_cutoff = 0.998, 3.4, 2.5
+    cfg = E.EngineConfig(1, maxnb, 16, 0, tpa, 0, reps, ff, thermo if thermo is not None else E.Thermostat())
+    return cfg, reps
+
+
+def test_engine_config_validation_is_host_side():
+    """acs_engine_bytes sizes the engine's device block on the host: it is positive for valid configurations
+    and 0 for invalid ones (threads per atom, list radius against the box, thermostat parameters)."""
+    from devinproj_b200 import engine as E
+    from devinproj_b200.engine import ENGINE_SIGNATURES
+    L = _lib.lib()
+    res, args = ENGINE_SIGNATURES["acs_engine_bytes"]
+    L.acs_engine_bytes.restype, L.acs_engine_bytes.argtypes = res, args
+    cfg, keep = _engine_config()
+    ok = L.acs_engine_bytes(C.byref(cfg))
+    assert ok > 864 * 96 * 4
+    for tpa in (2, 4, 8, 16, 32):
+        c2, k2 = _engine_config(tpa=tpa)
+        assert L.acs_engine_bytes(C.byref(c2)) > 0
+    bad = [_engine_config(tpa=3), _engine_config(box_sigma=5.0),   # rlist must stay below box / 2
+           _engine_config(thermo=E.Thermostat(3, 0, 1.0, 1.0, 0, 0.0)),
+           _engine_config(thermo=E.Thermostat(1, 0, 1.0, -1.0, 0, 0.0)),
+           _engine_config(thermo=E.Thermostat(2, 0, 1.0, 0.0, 0, 0.0))]
+    for c3, k3 in bad:
+        assert L.acs_engine_bytes(C.byref(c3)) == 0
+    good = [E.Thermostat(1, 0, 0.997, 0.05, 7, 0.0), E.Thermostat(2, 0, 0.997, 0.0, 0, 2.0)]
+    for th in good:
+        c4, k4 = _engine_config(thermo=th)
+        assert L.acs_engine_bytes(C.byref(c4)) >= ok
+
+
+def test_rdf_workspace_query():
+    g = _lib.AcsGrid()
+    box = np.full(3, 30.0)
+    assert _lib.lib().acs_grid_setup(C.byref(g), box.ctypes.data, 1, None, None, 14.0) == 0
+    assert _lib.lib().acs_rdf_work_bytes(1000, C.byref(g)) == _lib.lib().acs_nlist_work_bytes(1000, C.byref(g)) > 0
