@@ -258,6 +258,7 @@ class Engine:
 
     def set_correction_stride(self, stride):
         _lib.check(self.L.acs_engine_set_correction_stride(self.h, int(stride)), "acs_engine_set_correction_stride")
+        self.c_stride = int(stride)
 
     def last_correction_ms(self):
         return float(self.L.acs_engine_last_correction_ms(self.h))
@@ -422,6 +423,8 @@ class GpuSimulation:
             raise ValueError("GpuSimulation integrates with VelocityVerlet, Langevin (BAOAB) or NoseHoover")
         thermo = (langevin_thermostat(integrator, seed) if kind == "Langevin"
                   else nose_hoover_thermostat(integrator) if kind == "NoseHoover" else None)
+        self._thermo = thermo
+        self._tpa, self._grid_mult = tpa, grid_mult
         self._nh = kind == "NoseHoover"
         self.system = system
         self.forces = list(forces)
@@ -545,13 +548,20 @@ class GpuSimulation:
             else:
                 block = min(re * max(1, min(eng.rec_cap - 1, 4000 // re)), left)
             periodic = 0 if (positions or off) else re
+            snap = eng.get_state()[:2]            # device copy: the block is redone from here on overflow
+            nh_snap = eng.nh_state() if self._nh else None
             eng.run(block, periodic, True)        # every block also records its last step
             local = list(range(periodic, block + 1, periodic)) if periodic else []
             if not local or local[-1] != block:
                 local.append(block)
+            try:
+                eng.check("engine run")
+            except _lib.ListOverflow:
+                self._regrow(eng.status().need_nbr, snap, nh_snap)
+                eng = self.engine
+                continue
             recs = eng.records(len(local))[:, 0, :]
             baths = eng.bath_records(len(local))[:, 0] if self._nh else np.zeros(len(local))
-            eng.check("engine run")
             kept = [(j, rec, b) for j, rec, b in zip(local, recs, baths) if (done + j) % re == 0 or done + j == steps]
             if positions and kept:
                 self._pull_positions()
@@ -572,6 +582,29 @@ class GpuSimulation:
         self._pull()
         self._sync_thermostat()
         return self.trajectory
+
+    def _regrow(self, need, snap, nh_snap):
+        """A neighbour list outgrew its capacity during a block (the engine stops its kernels then): build an
+        engine with room for the largest list plus 20%, restore the block's start state and thermostat state,
+        and let the caller redo the block. A Langevin run continues with the new engine's draws."""
+        old = self.engine
+        pos, vel = snap
+        self.system.pos = np.mod(pos.cpu().numpy() * LEN, self.system.box)
+        self.system.vel = vel.cpu().numpy() * VEL
+        maxnb = int(max(need, old.maxnb) * 1.2 + 16 + 7) // 8 * 8
+        self.engine, self.rlist, self.half_skin = start_engine(
+            [self.system], self.forces, [self.dt], maxnb=maxnb, rec_cap=old.rec_cap, grid_mult=self._grid_mult,
+            tpa=old.tpa, thermo=self._thermo)
+        self.engine.set_correction_stride(getattr(old, "c_stride", 1))
+        if nh_snap is not None:
+            self.engine.set_nh_state(nh_snap)
+            _upload_state(self.engine, [self.system])
+        if self.correction is not None:
+            self.engine.set_correction(self.correction, True)
+            _upload_state(self.engine, [self.system])
+        self.engine.check("regrown engine")
+        self.regrowths = getattr(self, "regrowths", 0) + 1
+        del old
 
     def _pull_positions(self):
         pos, vel, _ = self.engine.get_state()

@@ -288,3 +288,19 @@ def test_engine_nose_hoover_conserves_extended_energy():
     assert coarse["thermostat"].status == "PASS", coarse["thermostat"]
     assert coarse["extended energy"].value < 1e-3
     assert coarse["extended energy"].value / fine["extended energy"].value > 2.5
+
+
+def test_list_overflow_mid_run_regrows_and_continues():
+    """The fcc argon lattice has exactly 78 neighbours per atom within the list radius, so a capacity of 80
+    holds the first lists; once the crystal melts, some atom's list outgrows it during a run. The run goes on
+    with a regrown engine from the block's start state, and the final forces match the FP64 oracle."""
+    from devinproj_b200 import GpuSimulation, configs
+    s, forces, dt = configs.argon864(seed=9)
+    s.vel *= np.sqrt(300.0 / s.temperature())
+    sim = GpuSimulation(s, forces, dt=dt, maxnb=80)
+    assert sim.engine.maxnb == 80
+    sim.run(steps=400, record_every=100, positions=False)
+    assert getattr(sim, "regrowths", 0) >= 1 and sim.engine.maxnb > 80
+    assert len(sim.trajectory.t) == 5
+    Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(oracle_of(s))
+    assert rms_rel(sim.force, Fo) <= 1e-5
