@@ -260,7 +260,6 @@ def main():
     eng.run(args.warmup, 0, True)
     torch.cuda.synchronize()
     eng.check("warm-up")
-    rb0 = eng.status().rebuilds
 
     def barrier():
         if world > 1:
@@ -270,6 +269,7 @@ def main():
     eng.run(args.steps, args.record_every, True)   # instantiate the graph outside the timed region
     torch.cuda.synchronize()
     eng.check("graph warm-up")
+    rb0 = eng.status().rebuilds
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         time.sleep(0.25)
