@@ -102,6 +102,8 @@ struct Eng {
   double* nh_st;                 // Nose-Hoover per replica: xi, eta, K2 for the next start half, scale to
                                  // apply, end-half scale (records), 3 spare (8 doubles)
   double* rec_bath;              // bath energy per record and replica
+  int32_t* fcell;                // per rebuild: prefix over replicas of the flagged cells the warp-per-cell
+                                 // list build covers (R + 1 entries)
   uint32_t seed_lo, seed_hi;
   unsigned long long* octr;      // O-steps taken so far (Langevin draws: counter)
 };
@@ -808,6 +810,24 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   }
   if (!any || err0) return;
   unsigned long long t_prev = (blockIdx.x == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
+  if (blockIdx.x == 0) {
+    // exclusive prefix of the cells the warp-per-cell list build visits (flagged replicas with >= 3 cells on
+    // every axis), so that its warps take only those cells, in turn (balanced when few replicas rebuild)
+    const int per = (E.R + blockDim.x - 1) / blockDim.x, r0 = threadIdx.x * per;
+    int sum = 0;
+    for (int r = r0; r < min(r0 + per, E.R); ++r) {
+      const RepDev& R = E.rep[r];
+      if (fl[r] && R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3) sum += R.ncells;
+    }
+    int total;
+    int ex = block_scan_excl(sum, &total);
+    for (int r = r0; r < min(r0 + per, E.R); ++r) {
+      E.fcell[r] = ex;
+      const RepDev& R = E.rep[r];
+      if (fl[r] && R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3) ex += R.ncells;
+    }
+    if (threadIdx.x == 0) E.fcell[E.R] = total;
+  }
 #define PHASE(k)                                                  \
   if (blockIdx.x == 0 && threadIdx.x == 0) {                      \
     const unsigned long long t_now = gtimer();                    \
@@ -1005,7 +1025,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       if (lane == 0) ps.finish(cnt);
     }
   } else {
-    // Replicas with >= 3 cells on every axis: a warp per home cell. The candidates of the 27 stencil cells, in
+    // Replicas with >= 3 cells on every axis: a warp per home cell (the warps take the flagged replicas' cells
+    // in turn, through the prefix block 0 wrote at the start). The candidates of the 27 stencil cells, in
     // list order (stencil cell, then ascending slot), are read 32 at a time with the cell pair's image shift
     // already added; those whose distance to the home cell's box exceeds the list radius (with the band
     // margin) cannot pair with any home atom and are dropped, the rest are compacted in order into a
@@ -1020,11 +1041,20 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int64_t c = gw; c < E.C; c += nw) {
-      const int r = E.cell_rep[c];
-      if (!fl[r]) continue;
+    const int nflag = __ldcg(E.fcell + E.R);   // written by block 0 in this launch: read through L2
+    for (int f = (int)gw; f < nflag; f += (int)nw) {
+      int r = 0;   // the replica whose range of the prefix holds f: the last r with fcell[r] <= f
+      for (int lo = 0, hi = E.R - 1; lo <= hi;) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldcg(E.fcell + mid) <= f) {
+          r = mid;
+          lo = mid + 1;
+        } else {
+          hi = mid - 1;
+        }
+      }
       const RepDev& R = E.rep[r];
-      if (R.nc[0] < 3 || R.nc[1] < 3 || R.nc[2] < 3 || c - R.cellbase >= R.ncells) continue;
+      const int64_t c = R.cellbase + (f - __ldcg(E.fcell + r));
       const float4* __restrict__ im = E.img[dst];
       const float rl2f = (float)R.rl2, lo_f = rl2f * (1.0f - 1e-4f), hi_f = rl2f * (1.0f + 1e-4f);
       // stencil cell st = 9 (a + 1) + 3 (b + 1) + (d + 1) in list order: lane st holds its first slot, its
@@ -1607,6 +1637,7 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(8 * (size_t)NCH);                    // 44 Nose-Hoover chunk partials
   L.add(8 * 8 * (size_t)R);                  // 45 Nose-Hoover state
   L.add(8 * (size_t)rec_cap * R);            // 46 bath-energy records
+  L.add(4 * ((size_t)R + 1));                // 47 flagged-cell prefix of a rebuild
   return L;
 }
 
@@ -1866,6 +1897,7 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.nh_chunk = (double*)(b + L.off[44]);
   E.nh_st = (double*)(b + L.off[45]);
   E.rec_bath = (double*)(b + L.off[46]);
+  E.fcell = (int32_t*)(b + L.off[47]);
   E.thermo = cfg->thermo.kind;
   E.seed_lo = (uint32_t)cfg->thermo.seed;
   E.seed_hi = (uint32_t)(cfg->thermo.seed >> 32);
