@@ -1962,7 +1962,12 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   }
   e->coop_blocks = sms * std::min(per_sm, 4);
   const int grid_mult = cfg->grid_mult > 0 ? cfg->grid_mult : 0;
-  const int64_t need = (S / G * 32 + 255) / 256;
+  // 128-thread step blocks when a 256-thread grid would fill fewer than two waves (4 blocks per SM): the
+  // blocks then spread more evenly over the SMs (4096-ion NaCl: step kernel 6% faster; at 1M atoms 256 is
+  // 0.3% faster)
+  const int64_t need256 = (S / G * 32 + 255) / 256;
+  e->step_threads = need256 < 2 * 4 * (int64_t)sms ? 128 : 256;
+  const int64_t need = (S / G * 32 + e->step_threads - 1) / e->step_threads;
   e->step_blocks = (int)(grid_mult ? std::min<int64_t>(need, (int64_t)sms * grid_mult) : need);
   if (e->step_blocks < 1) e->step_blocks = 1;
   *out = e;
