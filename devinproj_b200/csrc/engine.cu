@@ -1960,7 +1960,12 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
     delete e;
     return ACS_ERR_CUDA;
   }
-  e->coop_blocks = sms * std::min(per_sm, 4);
+  // rebuild grid: at most 4 blocks per SM, and no more blocks than the largest phase can use (the list build
+  // takes a warp per cell, or a warp per slot at >= 8 threads per atom; the other phases a thread per slot),
+  // since each of its grid barriers costs in proportion to the blocks (small systems)
+  const int64_t list_warps = tpa >= 8 ? S : (int64_t)C;
+  const int64_t useful = std::max<int64_t>((S + 255) / 256, (list_warps + 7) / 8);
+  e->coop_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * std::min(per_sm, 4), useful));
   const int grid_mult = cfg->grid_mult > 0 ? cfg->grid_mult : 0;
   // 128-thread step blocks when a 256-thread grid would fill fewer than two waves (4 blocks per SM): the
   // blocks then spread more evenly over the SMs (4096-ion NaCl: step kernel 6% faster; at 1M atoms 256 is
