@@ -101,6 +101,41 @@ def test_engine_lists_stay_valid_across_rebuilds():
     assert abs(sim.pe - Uo) <= 2e-6 * abs(Uo)
 
 
+def test_engine_full_size_lj1m_pair_set_forces_and_net_force():
+    """The headline system at full size (1,048,576-atom LJ fluid, fcc 64^3, rho* 0.8442, T* 0.72), through
+    size-independent properties, on the displaced lattice and again on the state after 200 steps (about 20
+    rebuilds): the engine's lists hold exactly twice the FP64 pair set at the list radius (the drop-in's
+    cell_list_pairs, itself pinned to the reference's pair sets); FP32c forces within the force tolerance of
+    the FP64 plug-in's on the same positions, energy within 2e-6, and the net force at round-off."""
+    from devinproj_b200 import GpuSimulation, cell_list_pairs, configs
+    from devinproj_b200.engine import forcefield_from
+    s, forces, dt = configs.lj_large(64)
+    assert s.n == 1_048_576
+    # the lattice's forces vanish by symmetry: displace every atom by a seeded 0.02 sigma first
+    s.pos = (s.pos + np.random.default_rng(7).normal(0, 0.02 * configs.AR_SIGMA, s.pos.shape)) % s.box
+    _, rlist, _ = forcefield_from(forces, s.species)
+    for stage in ("initial", "after 200 steps"):
+        sim = GpuSimulation(s, forces, dt=dt)
+        i, j = cell_list_pairs(s, rlist)
+        assert sim.engine.neighbor_stats()[1] == 2 * len(i), stage
+        F64 = np.zeros_like(s.pos)
+        U64 = 0.0
+        for f in forces:
+            Fi, Ui = f.compute(s)
+            F64 += Fi
+            U64 += Ui
+        e = rms_rel(sim.force, F64)
+        print(f"1M LJ {stage}: FP32c force RMS rel error {e:.2e}, energy rel error {abs(sim.pe - U64) / abs(U64):.2e}")
+        assert e <= 1e-5, stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+        frms = np.sqrt(np.mean(np.sum(F64 ** 2, 1)))
+        assert np.linalg.norm(sim.force.sum(0)) <= 1e-6 * np.sqrt(s.n) * frms, stage
+        if stage == "initial":
+            sim.run(steps=200, record_every=100, positions=False)
+            assert sim.rebuilds >= 10
+        del sim
+
+
 def test_batched_replicas_equal_single_runs_bitwise():
     """Replicas of different sizes and dt in one engine advance exactly as each would alone."""
     from devinproj_b200 import configs
