@@ -39,6 +39,7 @@ constexpr int kChunkTiles = 64; // record-reduction chunk, in atom groups (G ato
 constexpr int kCellChunk = 1024;  // cell-scan chunk (4 cells per thread of a 256-thread block)
 constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
+constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
 constexpr long long kSpinLimit = 20000000;  // ~2 s of 100 ns sleeps
 
 struct RepDev {
@@ -104,6 +105,11 @@ struct Eng {
   double* rec_bath;              // bath energy per record and replica
   int32_t* fcell;                // per rebuild: prefix over replicas of the flagged cells the warp-per-cell
                                  // list build covers (R + 1 entries)
+  const int32_t* ex_start;       // DSF exclusions by atom index within a replica (CSR), or none
+  const int32_t* ex_ids;
+  int32_t n_ex_ids;
+  uint32_t ex_bit;               // list-entry flag of an excluded pair (bit 26), 0 without exclusions
+  uint32_t jmask;                // slot bits of a list entry: 26 with exclusions, else 27
   uint32_t seed_lo, seed_hi;
   unsigned long long* octr;      // O-steps taken so far (Langevin draws: counter)
 };
@@ -257,7 +263,7 @@ __device__ __forceinline__ PairK pair_consts(const FFDev& ff, int p, const PairK
 template <bool LJ, bool DSF, bool REC, bool ONE, bool KAHAN = true>
 __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int sio, const float4& pi, uint32_t e,
                                           const float4& pj, const float4* shift_row, float& fx, float& fy, float& fz,
-                                          float& cx, float& cy, float& cz, float& eu, float& ce) {
+                                          float& cx, float& cy, float& cz, float& eu, float& ce, uint32_t exb) {
   const float4 sh = shift_row[e >> kIdxBits];
   const float dx = (pj.x - pi.x) + sh.x;
   const float dy = (pj.y - pi.y) + sh.y;
@@ -274,7 +280,7 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
     if (REC && in) kahan_add(eu, ce, k.eps4 * (sr6 * sr6 - sr6) - k.ushift);
   }
   if (DSF) {
-    if (r2 < ff.dsf_rc2) {
+    if (r2 < ff.dsf_rc2 && !(e & exb)) {   // excluded pairs (flag exb) have no DSF term
       const float ir = rsqrtf(r2);
       const float rr = r2 * ir;
       const float ar = ff.dsf_a * rr;
@@ -335,6 +341,8 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
   const int wpb = blockDim.x >> 5;
   if (E.status->flags & (ACS_FLAG_OVERFLOW | ACS_FLAG_NONFINITE | ACS_FLAG_TIMEOUT)) return;
   const float4* __restrict__ imgs = E.img[src];
+  // slot bits of a list entry and the DSF exclusion flag (entries of the LJ-only kernel carry no flag)
+  const uint32_t jm = DSF ? E.jmask : kIdxMask, exb = DSF ? E.ex_bit : 0u;
   const int G = E.G, tpa = E.tpa;
   const int sub_i = lane % G, phase = lane / G;
   PairK c1;
@@ -387,7 +395,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
 #pragma unroll
         for (int q = 0; q < 4; ++q) e[q] = en[q];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & kIdxMask));
+        for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & jm));
         if (t + 4 < n4) {
 #pragma unroll
           for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + (t + 4 + q) * 32);
@@ -396,15 +404,16 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         float bx = 0.f, by = 0.f, bz = 0.f, bcx, bcy, bcz;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          pair_term<LJ, DSF, REC, ONE, false>(ff, c1, sio, pi, e[q], pj[q], shift_row, bx, by, bz, bcx, bcy, bcz, eu, ce);
+          pair_term<LJ, DSF, REC, ONE, false>(ff, c1, sio, pi, e[q], pj[q], shift_row, bx, by, bz, bcx, bcy, bcz, eu, ce,
+                                              exb);
         kahan_add(fx, cx, bx);
         kahan_add(fy, cy, by);
         kahan_add(fz, cz, bz);
       }
       for (; t < n_it; ++t) {
         const uint32_t e = (uint32_t)ld_list(lst + t * 32);
-        const float4 pj = __ldg(imgs + (e & kIdxMask));
-        pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e, pj, shift_row, fx, fy, fz, cx, cy, cz, eu, ce);
+        const float4 pj = __ldg(imgs + (e & jm));
+        pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e, pj, shift_row, fx, fy, fz, cx, cy, cz, eu, ce, exb);
       }
       dfx = (double)fx - (double)cx;
       dfy = (double)fy - (double)cy;
@@ -656,6 +665,15 @@ __device__ int block_scan_excl(int v, int* total) {
   return ex;
 }
 
+// DSF exclusion of the pair of atoms (a, b), indices within their replica: b among a's excluded atoms
+// (accusim/forces.py:418-426).
+__device__ __forceinline__ bool dsf_excluded(const Eng& E, int32_t a, int32_t b) {
+  if ((uint32_t)a >= (uint32_t)E.n_ex_ids) return false;
+  for (int32_t q = E.ex_start[a]; q < E.ex_start[a + 1]; ++q)
+    if (E.ex_ids[q] == b) return true;
+  return false;
+}
+
 // Per-atom state of the list build: stencil ranges, FP32 screen and the exact FP64 decision.
 struct PairScan {
   const Eng& E;
@@ -772,7 +790,9 @@ __device__ __noinline__ bool band_accept(const double* __restrict__ xa, int64_t 
 }
 
 // Rebuild of flagged replicas and per-replica record reduction. Cooperative launch (all blocks resident);
-// every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging.
+// every wait is bounded and reports ACS_FLAG_TIMEOUT instead of hanging. EX: the engine has DSF exclusions
+// (excluded pairs' list entries get the flag E.ex_bit).
+template <bool EX>
 __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int rec_idx, int force_all) {
   __shared__ unsigned char fl[kMaxRep];
   __shared__ int any_s;
@@ -1026,7 +1046,11 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
               if (k < k1 && k != i) code = ps.test(k, a, b, d);
               const unsigned bal = __ballot_sync(0xffffffffu, code >= 0);
               const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-              if (code >= 0 && pos < E.maxnb) ps.lst[(int64_t)pos * E.G] = (int32_t)((uint32_t)k | ((uint32_t)code << kIdxBits));
+              if (code >= 0 && pos < E.maxnb) {
+                uint32_t v = (uint32_t)k | ((uint32_t)code << kIdxBits);
+                if (EX && dsf_excluded(E, E.id[i], E.id[k])) v |= E.ex_bit;
+                ps.lst[(int64_t)pos * E.G] = (int32_t)v;
+              }
               cnt += __popc(bal);
             }
           }
@@ -1182,7 +1206,11 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           while (m_in) {   // list order
             const int t = __ffs(m_in) - 1;
             m_in &= m_in - 1u;
-            if (cnt < E.maxnb) lst[(int64_t)cnt * E.G] = (int32_t)bufk[wib][t];
+            if (cnt < E.maxnb) {
+              uint32_t v = bufk[wib][t];
+              if (EX && dsf_excluded(E, E.id[i], E.id[v & kIdxMask])) v |= E.ex_bit;
+              lst[(int64_t)cnt * E.G] = (int32_t)v;
+            }
             ++cnt;
           }
           // keep the survivors beyond this batch at the front of the buffer
@@ -1232,7 +1260,11 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
                 if (k + t < k1 && k + t != i && q[t] < ps.hi_f) {
                   const int code = q[t] <= ps.lo_f && !ps.any_one ? ps.scode(a, b, d) : ps.test(k + t, a, b, d);
                   if (code >= 0) {
-                    if (cnt < E.maxnb) ps.lst[(int64_t)cnt * E.G] = (int32_t)((uint32_t)(k + t) | ((uint32_t)code << kIdxBits));
+                    if (cnt < E.maxnb) {
+                      uint32_t v = (uint32_t)(k + t) | ((uint32_t)code << kIdxBits);
+                      if (EX && dsf_excluded(E, E.id[i], E.id[k + t])) v |= E.ex_bit;
+                      ps.lst[(int64_t)cnt * E.G] = (int32_t)v;
+                    }
                     ++cnt;
                   }
                 }
@@ -1330,7 +1362,7 @@ __global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out)
     const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
     for (int k = 0; k < E.nnb[i]; ++k) {
       const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
-      const float4 pj = E.img[src][e & kIdxMask];
+      const float4 pj = E.img[src][e & E.jmask];
       const uint32_t code = e >> kIdxBits;
       const int mx = (int)(code % 3) - 1, my = (int)((code / 3) % 3) - 1, mz = (int)(code / 9) - 1;
       const float dx = (pj.x - pi.x) + mx * R.csf[0];
@@ -1339,7 +1371,7 @@ __global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out)
       const float r2 = dx * dx + dy * dy + dz * dz;
       const int p = sio + __float_as_int(pj.w);
       if (ff.lj && r2 < ff.lj_rc2[p]) ++nl;
-      if (ff.dsf && r2 < ff.dsf_rc2) ++nd;
+      if (ff.dsf && r2 < ff.dsf_rc2 && !(e & E.ex_bit)) ++nd;
     }
   }
   atomicAdd(out, nl);
@@ -1394,7 +1426,7 @@ __global__ void __launch_bounds__(256, 4) k_desc_engine(Eng E, int src, DescP P,
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
         const int k = base + 32 * u + lane;
-        pj[u] = k < m ? im[e[u] & kIdxMask] : make_float4(0.f, 0.f, 0.f, 0.f);
+        pj[u] = k < m ? im[e[u] & E.jmask] : make_float4(0.f, 0.f, 0.f, 0.f);
       }
       // species 0 staged from the front, species 1 from the back, each in list order
       int cnt0 = 0, cnt1 = 0;
@@ -1588,15 +1620,29 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     C += (int32_t)ncell + 1;
     NCH += R.nchunks;
     T = (int32_t)(S / 32);
-    if (S >= (int64_t)kIdxMask || C > INT32_MAX / 2) {
+    if (S >= (int64_t)kIdxMask || C > INT32_MAX / 2 || (cfg->n_ex_ids > 0 && S >= (int64_t)kExBit)) {
       err = ACS_ERR_UNSUPPORTED;
+      return;
+    }
+  }
+  if (cfg->n_ex_ids < 0 || (cfg->n_ex_ids > 0 && (!cfg->ex_start || !cfg->ex_ids || cfg->ex_start[0] != 0))) {
+    err = ACS_ERR_ARG;
+    return;
+  }
+  for (int32_t a = 0; a < cfg->n_ex_ids; ++a) {
+    if (cfg->ex_start[a + 1] < cfg->ex_start[a]) {
+      err = ACS_ERR_ARG;
       return;
     }
   }
 }
 
+int32_t ex_count(const acs_engine_config* cfg) {
+  return cfg->n_ex_ids > 0 && cfg->ex_start ? cfg->ex_start[cfg->n_ex_ids] : 0;
+}
+
 Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int32_t NCC, int32_t maxnb,
-                   int32_t rec_cap, int64_t NG) {
+                   int32_t rec_cap, int64_t NG, int32_t n_ex_ids, int32_t n_ex) {
   Layout L;
   L.add(sizeof(RepDev) * R);                 // 0 rep
   L.add(4 * (size_t)R);                      // 1 active
@@ -1646,6 +1692,8 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(8 * 8 * (size_t)R);                  // 45 Nose-Hoover state
   L.add(8 * (size_t)rec_cap * R);            // 46 bath-energy records
   L.add(4 * ((size_t)R + 1));                // 47 flagged-cell prefix of a rebuild
+  L.add(4 * ((size_t)n_ex_ids + 1));         // 48 DSF exclusions: CSR starts by atom id
+  L.add(4 * ((size_t)n_ex + 1));             // 49 DSF exclusions: excluded ids
   return L;
 }
 
@@ -1768,7 +1816,8 @@ int launch_rebuild(acs_engine* e, int dst, int rec, int rec_idx, int force_all, 
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t err = cudaLaunchKernelEx(&cfg, k_rebuild, e->E, dst, rec, rec_idx, force_all);
+  cudaError_t err = e->E.ex_bit ? cudaLaunchKernelEx(&cfg, k_rebuild<true>, e->E, dst, rec, rec_idx, force_all)
+                                 : cudaLaunchKernelEx(&cfg, k_rebuild<false>, e->E, dst, rec, rec_idx, force_all);
   return err == cudaSuccess ? ACS_OK : ACS_ERR_CUDA;
 }
 
@@ -1815,7 +1864,7 @@ size_t acs_engine_bytes(const acs_engine_config* cfg) {
   plan(cfg, reps, src0, S, T, C, NCH, NCC, err);
   if (err) return 0;
   return make_layout(cfg->n_replicas, S, T, C, NCH, NCC, cfg->maxnb, std::max(cfg->rec_cap, 1),
-                     S / (32 / tpa_of(cfg))).total;
+                     S / (32 / tpa_of(cfg)), cfg->n_ex_ids, ex_count(cfg)).total;
 }
 
 int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs_engine** out) {
@@ -1840,7 +1889,8 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   const int rec_cap = std::max(cfg->rec_cap, 1);
   const int tpa = tpa_of(cfg);
   const int G = 32 / tpa;
-  Layout L = make_layout(cfg->n_replicas, S, T, C, NCH, NCC, cfg->maxnb, rec_cap, S / G);
+  Layout L = make_layout(cfg->n_replicas, S, T, C, NCH, NCC, cfg->maxnb, rec_cap, S / G, cfg->n_ex_ids,
+                         ex_count(cfg));
   if (bytes < L.total) {
     delete e;
     return ACS_ERR_WORKSPACE;
@@ -1906,6 +1956,11 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.nh_st = (double*)(b + L.off[45]);
   E.rec_bath = (double*)(b + L.off[46]);
   E.fcell = (int32_t*)(b + L.off[47]);
+  E.n_ex_ids = cfg->n_ex_ids;
+  E.ex_start = (const int32_t*)(b + L.off[48]);
+  E.ex_ids = (const int32_t*)(b + L.off[49]);
+  E.ex_bit = cfg->n_ex_ids > 0 ? kExBit : 0u;
+  E.jmask = cfg->n_ex_ids > 0 ? kExBit - 1u : kIdxMask;
   E.thermo = cfg->thermo.kind;
   E.seed_lo = (uint32_t)cfg->thermo.seed;
   E.seed_hi = (uint32_t)(cfg->thermo.seed >> 32);
@@ -1943,6 +1998,13 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   ok = ok && cudaMemcpy(E.chunk_tile0, chunk_t0.data(), 4 * (size_t)NCH, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.chunk_ntiles, chunk_nt.data(), 4 * (size_t)NCH, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.status, &st0, sizeof(st0), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (cfg->n_ex_ids > 0) {
+    ok = ok && cudaMemcpy((void*)E.ex_start, cfg->ex_start, 4 * ((size_t)cfg->n_ex_ids + 1), cudaMemcpyHostToDevice) ==
+                   cudaSuccess;
+    const int32_t nnz = ex_count(cfg);
+    if (nnz > 0)
+      ok = ok && cudaMemcpy((void*)E.ex_ids, cfg->ex_ids, 4 * (size_t)nnz, cudaMemcpyHostToDevice) == cudaSuccess;
+  }
   ok = ok && cudaMemcpy(E.bar, bar0, 16, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(e->src0_dev, e->src0.data(), 8 * (size_t)E.R, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.cc_rep, cc_rep.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1955,7 +2017,8 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   ok = ok && cudaMemset(E.rec_bath, 0, 8 * (size_t)E.rec_cap * E.R) == cudaSuccess;
   int sms = 0, per_sm = 0;
   ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev) == cudaSuccess;
-  ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, 256, 0) == cudaSuccess;
+  ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, E.ex_bit ? k_rebuild<true> : k_rebuild<false>,
+                                                           256, 0) == cudaSuccess;
   if (!ok || per_sm < 1) {
     delete e;
     return ACS_ERR_CUDA;

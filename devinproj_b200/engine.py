@@ -53,7 +53,8 @@ class Thermostat(C.Structure):
 class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
                 ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
-                ("thermo", Thermostat)]
+                ("thermo", Thermostat), ("ex_start", C.POINTER(C.c_int32)), ("ex_ids", C.POINTER(C.c_int32)),
+                ("n_ex_ids", C.c_int32), ("pad2", C.c_int32)]
 
 
 def langevin_thermostat(integrator, seed):
@@ -135,8 +136,6 @@ def forcefield_from(forces, species) -> tuple[ForceField, float, float]:
         radii.append((f.cutoff * smax, f.cutoff * smax + f.skin * smax))
     if dsf:
         f = dsf[0]
-        if f.exclude:
-            raise ValueError("the engine does not take DSF exclusions; use the drop-in plug-ins")
         ff.dsf = 1
         ff.dsf_alpha = f.alpha * LEN
         ff.dsf_rcut = f.rcut / LEN
@@ -156,7 +155,7 @@ class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
     def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
-                 thermo=None):
+                 thermo=None, exclusions=None):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -175,6 +174,12 @@ class Engine:
         self.tpa = int(tpa)
         self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff,
                                 thermo if thermo is not None else Thermostat())
+        self._ex = exclusions   # (ex_start, ex_ids) int32 arrays, kept alive with the config
+        if exclusions is not None:
+            ex_start, ex_ids = exclusions
+            self.cfg.ex_start = ex_start.ctypes.data_as(C.POINTER(C.c_int32))
+            self.cfg.ex_ids = ex_ids.ctypes.data_as(C.POINTER(C.c_int32))
+            self.cfg.n_ex_ids = len(ex_start) - 1
         nbytes = L.acs_engine_bytes(C.byref(self.cfg))
         if nbytes == 0:
             raise ValueError("engine configuration rejected (sizes, list radius >= box/2, or too many replicas)")
@@ -348,7 +353,32 @@ def default_tpa(n_atoms_total, neighbors_per_atom):
     return tpa
 
 
-def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None):
+def dsf_exclusions(forces, systems):
+    """The DampedShiftedCoulomb exclusion id pairs as the engine takes them: CSR (ex_start, ex_ids) by atom
+    index, both directions, ids mapped to indices through `system.ids` as accusim/forces.py:418-419 does
+    (pairs with an id not in the system are dropped); None without exclusions. The engine applies one table
+    to every replica, so the replicas must number their atoms alike."""
+    dsf = [f for f in forces if type(f).__name__ == "DampedShiftedCoulomb"]
+    if not dsf or not dsf[0].exclude:
+        return None
+    ids = np.asarray(systems[0].ids)
+    for s in systems[1:]:
+        if not np.array_equal(np.asarray(s.ids), ids):
+            raise ValueError("DSF exclusions need the same atom ids in every replica")
+    where = {int(pid): k for k, pid in enumerate(ids)}
+    pairs = np.array([(where[a], where[b]) for a, b in dsf[0].exclude if a in where and b in where],
+                     dtype=np.int64).reshape(-1, 2)
+    if not len(pairs):
+        return None
+    a = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    b = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    order = np.argsort(a, kind="stable")
+    ex_start = np.concatenate([[0], np.cumsum(np.bincount(a, minlength=len(ids)))]).astype(np.int32)
+    return ex_start, np.ascontiguousarray(b[order], dtype=np.int32)
+
+
+def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None,
+                 exclusions=None):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -359,7 +389,8 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
         maxnb = expect
     if tpa is None:
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3)
-    return Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo), rlist, half_skin
+    return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
+                   exclusions=exclusions), rlist, half_skin)
 
 
 def _upload_state(engine, systems):
@@ -386,9 +417,10 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=
         from .autotune import tune
         tpa, grid_mult = tune(systems, forces, dts)
     reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
+    ex = dsf_exclusions(forces, systems)
     for attempt in range(3):
         eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,
-                                      tpa=tpa, thermo=thermo)
+                                      tpa=tpa, thermo=thermo, exclusions=ex)
         _upload_state(eng, systems)
         st = eng.status()
         if st.flags & _lib.FLAG_OVERFLOW:

@@ -67,6 +67,15 @@ typedef struct acs_engine_config {
   const acs_replica* replicas;  /* host array */
   acs_forcefield ff;
   acs_thermostat thermo;        /* zero: VelocityVerlet */
+  /* DampedShiftedCoulomb exclusions (accusim/forces.py:400, 418-426: atom pairs with no DSF interaction;
+   * the LJ term stays), the same for every replica, as host arrays in CSR form by atom index within a
+   * replica (the caller's order): the atoms excluded for atom a are ex_ids[ex_start[a] .. ex_start[a + 1]),
+   * listed from both sides. n_ex_ids = 0 (NULL arrays): none. With exclusions an engine holds fewer than
+   * 2^26 atom slots. */
+  const int32_t* ex_start;      /* n_ex_ids + 1 entries, ex_start[0] = 0, non-decreasing */
+  const int32_t* ex_ids;        /* ex_start[n_ex_ids] entries */
+  int32_t n_ex_ids;
+  int32_t pad2;
 } acs_engine_config;
 
 typedef struct acs_engine acs_engine;

@@ -108,6 +108,47 @@ def test_engine_config_validation_is_host_side():
         assert L.acs_engine_bytes(C.byref(c4)) >= ok
 
 
+def test_engine_dsf_exclusion_tables():
+    """DSF exclusions: the engine's CSR table by atom index (ids mapped through system.ids, both directions,
+    pairs with an unknown id dropped) and its host-side validation in acs_engine_bytes."""
+    from devinproj_b200 import DampedShiftedCoulomb, System
+    from devinproj_b200 import engine as E
+    from devinproj_b200.engine import ENGINE_SIGNATURES, dsf_exclusions
+    s = System(3, box=20.0, periodic=True)
+    s.add_species("Na", 1.0, charge=1.0)
+    s.add("Na", np.random.default_rng(0).uniform(0, 20, (6, 3)))
+    s.ids = np.array([10, 11, 12, 13, 14, 15])
+    f = DampedShiftedCoulomb(rcut=3.0, exclude=[(10, 12), (15, 11), (12, 13), (99, 10)])
+    ex_start, ex_ids = dsf_exclusions([f], [s])
+    got = {a: sorted(ex_ids[ex_start[a]:ex_start[a + 1]].tolist()) for a in range(6)}
+    assert got == {0: [2], 1: [5], 2: [0, 3], 3: [2], 4: [], 5: [1]}
+    assert dsf_exclusions([DampedShiftedCoulomb(rcut=3.0)], [s]) is None
+    s2 = s.copy()
+    s2.ids = np.array([10, 11, 12, 13, 15, 14])
+    with pytest.raises(ValueError):
+        dsf_exclusions([f], [s, s2])
+
+    L = _lib.lib()
+    res, args = ENGINE_SIGNATURES["acs_engine_bytes"]
+    L.acs_engine_bytes.restype, L.acs_engine_bytes.argtypes = res, args
+    base, keep = _engine_config()
+    n0 = L.acs_engine_bytes(C.byref(base))
+    cfg, keep = _engine_config()
+    cfg.ex_start = ex_start.ctypes.data_as(C.POINTER(C.c_int32))
+    cfg.ex_ids = ex_ids.ctypes.data_as(C.POINTER(C.c_int32))
+    cfg.n_ex_ids = 6
+    assert L.acs_engine_bytes(C.byref(cfg)) >= n0 > 0
+    for start in (np.array([1, 1, 2, 4, 5, 5, 6], np.int32), np.array([0, 2, 1, 4, 5, 5, 6], np.int32)):
+        bad, keep2 = _engine_config()
+        bad.ex_start = start.ctypes.data_as(C.POINTER(C.c_int32))
+        bad.ex_ids = ex_ids.ctypes.data_as(C.POINTER(C.c_int32))
+        bad.n_ex_ids = 6
+        assert L.acs_engine_bytes(C.byref(bad)) == 0
+    nul, keep3 = _engine_config()
+    nul.n_ex_ids = 6
+    assert L.acs_engine_bytes(C.byref(nul)) == 0
+
+
 def test_rdf_workspace_query():
     g = _lib.AcsGrid()
     box = np.full(3, 30.0)

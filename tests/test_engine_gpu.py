@@ -53,6 +53,36 @@ def test_engine_nacl_lj_dsf_forces_vs_reference(golden):
     assert abs(sim.pe - Uref) <= 2e-6 * abs(Uref)
 
 
+@pytest.mark.parametrize("tpa", [1, 32])
+def test_engine_dsf_exclusions_match_fp64_plugins(golden, tpa):
+    """DSF exclusions in the engine (accusim/forces.py:400, 418-426): 4096-ion NaCl with 600 close ion pairs
+    excluded from the Coulomb term (LJ kept), against the FP64 plug-ins with the same exclusions (pinned to
+    the reference by the exclusion golden test), on the start state and after 200 steps (rebuilds re-sort
+    the atoms), with the list built by a warp per cell (1 thread per atom) and by a warp per atom (32)."""
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones, cell_list_pairs
+    g = golden("nacl4096")
+    s = product_system(g)
+    params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+    i, j = cell_list_pairs(s, 3.2e-10)
+    pick = np.random.default_rng(3).choice(len(i), 600, replace=False)
+    exclude = [(int(s.ids[a]), int(s.ids[b])) for a, b in zip(i[pick], j[pick])]
+    lj = LennardJones(params, cutoff=2.5)
+    dsf = DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"]), exclude=exclude)
+    sim = GpuSimulation(s, [lj, dsf], dt=float(g["dt"]), tpa=tpa)
+    for stage in ("start", "after 200 steps"):
+        if stage != "start":
+            sim.run(steps=200, record_every=100, positions=False)
+        F64 = lj.compute(s)[0] + dsf.compute(s)[0]
+        U64 = lj.compute(s)[1] + dsf.compute(s)[1]
+        F_noex = lj.compute(s)[0] + DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"])).compute(s)[0]
+        assert rms_rel(F_noex, F64) > 1e-2           # the exclusions matter at this tolerance
+        e = rms_rel(sim.force, F64)
+        print(f"nacl4096 with exclusions, tpa {tpa}, {stage}: force RMS rel error {e:.2e}")
+        assert e <= 1e-5, stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+    assert sim.rebuilds >= 2
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
@@ -174,8 +204,8 @@ def test_engine_rejects_unsupported_setups():
     s3 = System(3, box=4e-9, periodic=True)
     s3.add_species("Na", 3.8e-26, charge=1.6e-19)
     s3.add("Na", [[0, 0, 0], [2e-10, 0, 0]])
-    with pytest.raises(ValueError):
-        GpuSimulation(s3, [DampedShiftedCoulomb(rcut=1e-9, exclude=[(0, 1)])], dt=1e-15)
+    with pytest.raises(ValueError):   # one DampedShiftedCoulomb at most
+        GpuSimulation(s3, [DampedShiftedCoulomb(rcut=1e-9), DampedShiftedCoulomb(rcut=1.1e-9)], dt=1e-15)
 
 
 @pytest.mark.parametrize("seed", [0, 5])
