@@ -240,6 +240,16 @@ __device__ bool grid_sync(unsigned int* bar, acs_dev_status* st) {
 }
 
 // ------------------------------------------------------------------------------- pair kernel --
+// erfc(x), x >= 0, from e = exp(-x^2): Abramowitz & Stegun 7.1.26 (Hastings' approximation, |error| <= 1.5e-7
+// in exact arithmetic), erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e with t = 1 / (1 + p x). Branch-free
+// and it reuses the exponential the DSF force needs anyway; FP32 evaluation stays within 7e-7 of erfc.
+__device__ __forceinline__ float erfc_as(float x, float e) {
+  const float t = rcp_approx(fmaf(0.3275911f, x, 1.0f));
+  const float q = fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f),
+                       0.254829592f);
+  return t * q * e;
+}
+
 // Per-pair coefficients: either the single-species constants (ONE) or the species-pair tables.
 struct PairK {
   float eps4, eps24, sig2, rc2, ushift, qqk;
@@ -279,15 +289,16 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
     coef = in ? -k.eps24 * ir2 * sr6 * (2.0f * sr6 - 1.0f) : 0.f;
     if (REC && in) kahan_add(eu, ce, k.eps4 * (sr6 * sr6 - sr6) - k.ushift);
   }
-  if (DSF) {
-    if (r2 < ff.dsf_rc2 && !(e & exb)) {   // excluded pairs (flag exb) have no DSF term
-      const float ir = rsqrtf(r2);
-      const float rr = r2 * ir;
-      const float ar = ff.dsf_a * rr;
-      const float er = erfcf(ar);
-      coef -= k.qqk * ((er * ir * ir + ff.dsf_c * __expf(-ar * ar) * ir) - ff.dsf_fshift) * ir;
-      if (REC) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
-    }
+  if (DSF) {  // evaluated for every entry and selected, as the LJ term; excluded pairs (flag exb) have none
+    const bool ind = r2 < ff.dsf_rc2 && !(e & exb);
+    const float ir = rsqrtf(r2);
+    const float rr = r2 * ir;
+    const float ar = ff.dsf_a * rr;
+    const float ex = __expf(-ar * ar);
+    const float er = erfc_as(ar, ex);
+    const float cd = k.qqk * ((er * ir * ir + ff.dsf_c * ex * ir) - ff.dsf_fshift) * ir;
+    coef -= ind ? cd : 0.f;
+    if (REC && ind) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
   }
   if (KAHAN) {
     kahan_fma(fx, cx, coef, dx);

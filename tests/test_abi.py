@@ -154,3 +154,23 @@ def test_rdf_workspace_query():
     box = np.full(3, 30.0)
     assert _lib.lib().acs_grid_setup(C.byref(g), box.ctypes.data, 1, None, None, 14.0) == 0
     assert _lib.lib().acs_rdf_work_bytes(1000, C.byref(g)) == _lib.lib().acs_nlist_work_bytes(1000, C.byref(g)) > 0
+
+
+def test_engine_erfc_approximation_bound():
+    """The FP32 DSF term's erfc (Abramowitz & Stegun 7.1.26, as written in csrc/engine.cu) against scipy's:
+    within the method's published 1.5e-7 in FP64, and within 7e-7 when evaluated in FP32 as the kernel does."""
+    from scipy.special import erfc
+    src = open(os.path.join(os.path.dirname(__file__), "..", "devinproj_b200", "csrc", "engine.cu")).read()
+    body = src[src.index("float erfc_as(float x, float e)"):]
+    body = body[:body.index("\n}")]
+    c = [float(v) for v in re.findall(r"(-?\d+\.\d+)f", body) if float(v) != 1.0]   # p, then a5 .. a1 (Horner)
+    p, a5, a4, a3, a2, a1 = c
+    x = np.linspace(0.0, 4.0, 400001)
+    t = 1.0 / (1.0 + p * x)
+    approx = t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) * np.exp(-x * x)
+    assert np.max(np.abs(approx - erfc(x))) <= 1.5e-7
+    f = np.float32
+    xf = x.astype(f)
+    tf = f(1) / (f(1) + f(p) * xf)
+    qf = tf * (f(a1) + tf * (f(a2) + tf * (f(a3) + tf * (f(a4) + tf * f(a5)))))
+    assert np.max(np.abs((qf * np.exp(-(xf * xf))).astype(np.float64) - erfc(x))) <= 7e-7
