@@ -421,10 +421,25 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         kahan_add(fy, cy, by);
         kahan_add(fz, cz, bz);
       }
-      for (; t < n_it; ++t) {
-        const uint32_t e = (uint32_t)ld_list(lst + t * 32);
-        const float4 pj = __ldg(imgs + (e & jm));
-        pair_term<LJ, DSF, REC, ONE>(ff, c1, sio, pi, e, pj, shift_row, fx, fy, fz, cx, cy, cz, eu, ce, exb);
+      if (t < n_it) {
+        // the last 1-3 entries as one more block, their loads issued together; the missing entries get no
+        // shift and a partner at 3e30, so r^2 overflows and both terms select zero
+        const int rem = n_it - t;
+        uint32_t e[4];
+        float4 pj[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = q < rem ? (uint32_t)ld_list(lst + (t + q) * 32) : (13u << kIdxBits);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          pj[q] = q < rem ? __ldg(imgs + (e[q] & jm)) : make_float4(3e30f, 3e30f, 3e30f, pi.w);
+        float bx = 0.f, by = 0.f, bz = 0.f, bcx, bcy, bcz;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          pair_term<LJ, DSF, REC, ONE, false>(ff, c1, sio, pi, e[q], pj[q], shift_row, bx, by, bz, bcx, bcy, bcz, eu, ce,
+                                              exb);
+        kahan_add(fx, cx, bx);
+        kahan_add(fy, cy, by);
+        kahan_add(fz, cz, bz);
       }
       dfx = (double)fx - (double)cx;
       dfy = (double)fy - (double)cy;
