@@ -344,11 +344,15 @@ def estimate_maxnb(n, box, rlist):
     return int(min(expected * 1.3 + 32, 4096) + 7) // 8 * 8
 
 
-def default_tpa(n_atoms_total, neighbors_per_atom):
-    """Threads per atom for the pair kernel: enough threads to fill the GPU (about 300k), no more lanes than
-    a quarter of the neighbour count per atom."""
+def default_tpa(n_atoms_total, neighbors_per_atom, n_cells_total=None):
+    """Threads per atom for the pair kernel, which also picks the list build (a warp per atom from 8 threads
+    per atom, else a warp per cell). Measured on a B200 (LJ fcc fluids of 864 to 1M atoms, 4096-ion NaCl):
+    with fewer than 512 cells the warp-per-cell build lacks parallelism, so 32 threads per atom (16 for long
+    DSF lists) win; otherwise 1 to 4 threads per atom, enough for about 65k threads."""
+    if n_cells_total is not None and n_cells_total < 512:
+        return 16 if neighbors_per_atom > 200 else 32
     tpa = 1
-    while tpa < 32 and n_atoms_total * tpa < 300_000 and tpa * 8 <= max(neighbors_per_atom, 1):
+    while tpa < 4 and n_atoms_total * tpa < 65536:
         tpa *= 2
     return tpa
 
@@ -388,7 +392,8 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
     if maxnb is None:
         maxnb = expect
     if tpa is None:
-        tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3)
+        cells = sum(int(np.prod([max(1, int(bx // r["rlist"])) for bx in r["box"]])) for r in reps)
+        tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3, cells)
     return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
                    exclusions=exclusions), rlist, half_skin)
 

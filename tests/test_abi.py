@@ -174,3 +174,16 @@ def test_engine_erfc_approximation_bound():
     tf = f(1) / (f(1) + f(p) * xf)
     qf = tf * (f(a1) + tf * (f(a2) + tf * (f(a3) + tf * (f(a4) + tf * f(a5)))))
     assert np.max(np.abs((qf * np.exp(-(xf * xf))).astype(np.float64) - erfc(x))) <= 7e-7
+
+
+def test_default_threads_per_atom_follow_measured_optima():
+    """The size heuristic for threads per atom (host only) picks the B200 optima measured for these systems:
+    few cells -> a warp per atom (16 for the long DSF lists of NaCl), otherwise 1-4 threads per atom."""
+    from devinproj_b200.engine import default_tpa
+    assert default_tpa(864, 78, 27) == 32            # argon 864, 3^3 cells
+    assert default_tpa(4000, 78, 216) == 32          # LJ fcc 10^3
+    assert default_tpa(4096, 370, 27) == 16          # NaCl 4096, LJ + DSF
+    assert default_tpa(16384, 78, 729) == 4          # LJ fcc 16^3
+    assert default_tpa(32000, 78, 1331) == 4         # LJ fcc 20^3 (2 and 4 measured alike)
+    assert default_tpa(108000, 78, 4913) == 1        # LJ fcc 30^3
+    assert default_tpa(1048576, 78, 54872) == 1      # the 1M-atom fluid
