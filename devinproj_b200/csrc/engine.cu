@@ -1203,7 +1203,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           const uint32_t hs = (ck & kIdxMask) - hlo;   // home index of this candidate, if it is a home atom
           if (lane < nk && hs < (uint32_t)nh) selfpos[wib][hs] = lane;
           uint32_t m_in = 0u, m_hi = 0u;
-#pragma unroll 2
+#pragma unroll 4
           for (int h = 0; h < nh; ++h) {
             const float4 hp = hpos[wib][h];
             const float x = cur.x - hp.x, y = cur.y - hp.y, z = cur.z - hp.z;
