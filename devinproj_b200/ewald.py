@@ -90,6 +90,8 @@ class Ewald(Force):
             raise ValueError("Ewald needs a 3D periodic box")
         if not np.any(q):
             return np.zeros_like(s.pos), 0.0
+        if abs(q.sum()) > 1e-9 * np.sum(np.abs(q)):   # the reference's order: checked before any work
+            raise ValueError("Ewald summation here requires a charge-neutral system")
         require_cuda()
         F, U = self.compute_device(s, to_dev(s.pos), q)
         return F.cpu().numpy(), float(U)

@@ -37,3 +37,28 @@ def test_msd_matches_reference(golden):
     tr, _ = bio.load(os.path.join(GOLDEN, "io_traj108.npz"))
     t, m = msd(tr, box=g["box"])
     assert np.array_equal(t, g["t"]) and np.array_equal(m, g["msd"])
+
+
+def test_error_behaviour_matches_reference():
+    """The reference's exceptions for the same misuse, raised before any device work (accusim/forces.py:360-367,
+    accusim/simulation.py:96-97)."""
+    import numpy as np
+    import pytest
+    from devinproj_b200 import Simulation, System
+    from devinproj_b200.ewald import Ewald
+    s = System(3)                                   # open boundaries
+    s.add_species("Na", 1.0, charge=1.0)
+    s.add_species("Cl", 1.0, charge=-1.0)
+    s.add("Na", [[0.0, 0.0, 0.0]])
+    s.add("Cl", [[1.0, 0.0, 0.0]])
+    with pytest.raises(ValueError, match="3D periodic"):
+        Ewald(k=1.0).compute(s)
+    p = System(3, box=4.0, periodic=True)
+    p.add_species("Na", 1.0, charge=1.0)
+    p.add("Na", [[0.0, 0.0, 0.0], [2.0, 0.0, 0.0]])
+    with pytest.raises(ValueError, match="charge-neutral"):
+        Ewald(k=1.0).compute(p)
+    sim = Simulation(p, [])
+    with pytest.raises(ValueError, match="set dt"):
+        sim.run(steps=1)
+    assert np.all(sim.force == 0)
