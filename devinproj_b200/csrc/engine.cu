@@ -2,8 +2,8 @@
 // batch of independent replicas advanced together, captured in CUDA graphs.
 //
 // Per step the graph runs two kernels:
-//   k_step    one thread per atom slot: Kahan-compensated FP32 LJ / DSF pair sum over the atom's full
-//             neighbour list -> FP64 acceleration -> second half-kick (step completed; records taken
+//   k_step    1 to 32 threads per atom slot: Kahan-compensated FP32 LJ / DSF pair sum over the atom's full
+//             neighbour list (DSF exclusions flagged in the entries) -> FP64 acceleration -> second half-kick (step completed; records taken
 //             here) -> first half-kick of the next step -> drift -> FP32 image for the next step ->
 //             displacement test that flags its replica for a list rebuild. (accusim/integrators.py:25-31
 //             with the two kicks of consecutive steps fused.)
@@ -15,8 +15,9 @@
 // Positions are held as FP64 offsets u from the origin of the cell the atom was binned into at the last
 // rebuild (continuous between rebuilds); the absolute wrapped position is py_mod(origin + u, box), as
 // accusim/system.py:124-129 keeps it. Pair displacements are d = (img_j - img_i) + m * cell, with the FP32
-// images img = float(u) and the integer image shift m in {-1,0,1}^3 stored with the neighbour index.
-// d_ji == -d_ij bitwise, so pair forces are exactly antisymmetric.
+// images img = float(u) and the integer image shift m in {-1,0,1}^3 stored with the neighbour index
+// (entry = slot | code << 27, code = (m0 + 1) + 3 (m1 + 1) + 9 (m2 + 1); with DSF exclusions bit 26 flags an
+// excluded pair and the slot takes 26 bits). d_ji == -d_ij bitwise, so pair forces are exactly antisymmetric.
 #include <cooperative_groups.h>
 #include <math.h>
 
