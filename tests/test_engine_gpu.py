@@ -83,6 +83,29 @@ def test_engine_dsf_exclusions_match_fp64_plugins(golden, tpa):
     assert sim.rebuilds >= 2
 
 
+def test_engine_dsf_exclusions_in_a_one_cell_box():
+    """DSF exclusions through the list build for boxes with fewer than 3 list cells per edge (per-axis minimum
+    image, a thread per atom): 1000-ion NaCl in a 31.5 A box, 150 close pairs excluded, against the FP64
+    plug-ins with the same exclusions, at the start and after 200 steps."""
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, cell_list_pairs, configs
+    s, (lj, _) = configs.nacl_melt(10, seed=4)
+    s.pos = (s.pos + np.random.default_rng(4).normal(0, 0.1e-10, s.pos.shape)) % s.box
+    i, j = cell_list_pairs(s, 3.2e-10)
+    pick = np.random.default_rng(5).choice(len(i), 150, replace=False)
+    exclude = [(int(s.ids[a]), int(s.ids[b])) for a, b in zip(i[pick], j[pick])]
+    dsf = DampedShiftedCoulomb(rcut=12e-10, alpha=0.2e10, exclude=exclude)
+    sim = GpuSimulation(s, [lj, dsf], dt=1e-15, tpa=1)
+    for stage in ("start", "after 200 steps"):
+        if stage != "start":
+            sim.run(steps=200, record_every=100, positions=False)
+        F64 = lj.compute(s)[0] + dsf.compute(s)[0]
+        U64 = lj.compute(s)[1] + dsf.compute(s)[1]
+        e = rms_rel(sim.force, F64)
+        print(f"nacl1000 one-cell box with exclusions, {stage}: force RMS rel error {e:.2e}")
+        assert e <= 1e-5, stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
