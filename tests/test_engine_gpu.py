@@ -106,6 +106,37 @@ def test_engine_dsf_exclusions_in_a_one_cell_box():
         assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
 
 
+def test_engine_lj_species_without_parameters_do_not_interact():
+    """accusim/forces.py:108-113, 144-155: a species absent from the LJ parameters has eps = 0 and no LJ
+    interaction, and the list radius uses sigma_max over interacting pairs only. A 2048-atom Ar/Kr/tracer
+    mixture (a third of the atoms a tracer species with no parameters), engine vs the FP64 plug-in, at the
+    start and after 100 steps."""
+    from devinproj_b200 import GpuSimulation, LennardJones, System, configs
+    rng = np.random.default_rng(9)
+    base, _ = configs.lj_fluid(8, seed=9)
+    s = System(3, box=base.box.copy(), periodic=True)
+    s.add_species("Ar", configs.AR_MASS)
+    s.add_species("Kr", 83.798 * 1.66053906660e-27)
+    s.add_species("X", 20.0 * 1.66053906660e-27)
+    kind = rng.permutation(np.repeat([0, 1, 2], [1024, 512, 512]))
+    pos = (base.pos + rng.normal(0, 0.05 * configs.AR_SIGMA, base.pos.shape)) % s.box
+    for k, name in enumerate(("Ar", "Kr", "X")):
+        s.add(name, pos[kind == k])
+    s.maxwell_boltzmann(86.4, rng)
+    lj = LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA), "Kr": (1.4 * configs.AR_EPS, 3.6e-10)}, cutoff=2.5)
+    sim = GpuSimulation(s, [lj], dt=5e-15)
+    for stage in ("start", "after 100 steps"):
+        if stage != "start":
+            sim.run(steps=100, record_every=50, positions=False)
+        F64, U64 = lj.compute(s)
+        assert np.all(F64[s.sp == 2] == 0)
+        e = rms_rel(sim.force, F64)
+        print(f"Ar/Kr/tracer mixture, {stage}: force RMS rel error {e:.2e}")
+        assert e <= 1e-5, stage
+        assert np.all(sim.force[s.sp == 2] == 0), stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
