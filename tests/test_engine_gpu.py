@@ -137,6 +137,32 @@ def test_engine_lj_species_without_parameters_do_not_interact():
         assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
 
 
+@pytest.mark.parametrize("nz,tpa", [(6, 1), (6, 32), (12, 1)])
+def test_engine_orthorhombic_boxes(nz, tpa):
+    """Boxes with unequal edges: an LJ fluid on a perturbed 28 x 19 x nz lattice (spacing 1.06 sigma; box 29.7
+    x 20.1 x 6.4 sigma has a one-cell axis, 12.7 sigma does not), engine vs the FP64 plug-in at the start and
+    after 100 steps, through the thread-per-atom (one-cell axis), warp-per-atom and warp-per-cell list builds."""
+    from devinproj_b200 import GpuSimulation, LennardJones, System, configs
+    rng = np.random.default_rng(nz + tpa)
+    a = 1.06 * configs.AR_SIGMA
+    n = np.array([28, 19, nz])
+    s = System(3, box=n * a, periodic=True)
+    s.add_species("Ar", configs.AR_MASS)
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in n], indexing="ij"), -1).reshape(-1, 3)
+    s.add("Ar", ((g + 0.5) * a + rng.normal(0, 0.05 * configs.AR_SIGMA, g.shape)) % s.box)
+    s.maxwell_boltzmann(86.4, rng)
+    lj = LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)
+    sim = GpuSimulation(s, [lj], dt=5e-15, tpa=tpa)
+    for stage in ("start", "after 100 steps"):
+        if stage != "start":
+            sim.run(steps=100, record_every=50, positions=False)
+        F64, U64 = lj.compute(s)
+        e = rms_rel(sim.force, F64)
+        print(f"box {np.round(s.box / configs.AR_SIGMA, 1)} sigma, tpa {tpa}, {stage}: force RMS rel error {e:.2e}")
+        assert e <= 1e-5, stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
