@@ -6,6 +6,7 @@ The .npz files it writes are committed; nothing at test time imports the referen
 
 Each case restates a reference test or example setup (file:line inside the accusim project):
   lj_mix_{periodic,open}  tests/test_forces.py:64-76   300 Ar + 200 Kr, 4 nm box
+  lj_mix_ortho            the same mixture in a periodic 4 x 3 x 5.2 nm box (unequal edges)
   argon864                examples/rahman_argon.py:19-30 geometry at the fcc 6^3 / L=10.229 sigma config
   lj500_skin              tests/test_nose_hoover.py:6-17, 51-60   skin == fresh list along a VV run
   dsf_rocksalt10          tests/test_dsf.py:55-61       DSF dense == cell path
@@ -55,13 +56,14 @@ def save(name, **kw):
     print(f"{name}: {os.path.getsize(path) / 1024:.0f} KiB")
 
 
-def lj_mix(periodic):
+def lj_mix(periodic, box=None, name=None):
     rng = np.random.default_rng(5)
-    s = System(3, box=Q(4, "nm"), periodic=periodic)
+    edges = np.full(3, 4e-9) if box is None else np.asarray(box, float)
+    s = System(3, box=Q(4, "nm") if box is None else edges, periodic=periodic)
     s.add_species("Ar", Q(39.948, "u"))
     s.add_species("Kr", Q(83.8, "u"))
-    s.add("Ar", rng.uniform(0, 4e-9, (300, 3)))
-    s.add("Kr", rng.uniform(0, 4e-9, (200, 3)))
+    s.add("Ar", rng.uniform(0, 1, (300, 3)) * edges)
+    s.add("Kr", rng.uniform(0, 1, (200, 3)) * edges)
     params = {"Ar": (1.65e-21, 3.4e-10), "Kr": (2.3e-21, 3.6e-10)}
     Fd, Ud = LennardJones(params, pairlist_threshold=10 ** 9).compute(s)
     lj = LennardJones(params, pairlist_threshold=2)
@@ -70,7 +72,7 @@ def lj_mix(periodic):
     smax = float(np.max(np.where(eps_t > 0, sig_t, 0)))
     rl = (lj.cutoff + lj.skin) * smax
     i, j = cell_list_pairs(s, rl)
-    save(f"lj_mix_{'periodic' if periodic else 'open'}", **state_arrays(s),
+    save(name or f"lj_mix_{'periodic' if periodic else 'open'}", **state_arrays(s),
          param_names=np.array(["Ar", "Kr"]), param_eps=np.array([1.65e-21, 2.3e-21]),
          param_sig=np.array([3.4e-10, 3.6e-10]), cutoff=2.5, skin=0.3,
          F_dense=Fd, U_dense=Ud, F_list=Fl, U_list=Ul, list_radius=rl,
@@ -267,10 +269,21 @@ def analysis_cases():
     print(f"io_traj108: {os.path.getsize(os.path.join(OUT, 'io_traj108.npz')) / 1024:.0f} KiB")
 
 
+CASES = {
+    "lj_mix": lambda: (lj_mix(True), lj_mix(False)),
+    "lj_mix_ortho": lambda: lj_mix(True, box=(4e-9, 3e-9, 5.2e-9), name="lj_mix_ortho"),
+}
+
+
 if __name__ == "__main__":
     print("reference accusim", accusim.__version__, "from", os.path.dirname(accusim.__file__))
+    if len(sys.argv) > 1:   # named cases only: python make_golden.py lj_mix_ortho
+        for name in sys.argv[1:]:
+            CASES[name]()
+        sys.exit(0)
     lj_mix(True)
     lj_mix(False)
+    CASES["lj_mix_ortho"]()
     argon864()
     lj500_skin()
     dsf_cases()

@@ -43,7 +43,7 @@ def _ties(s, keys_a, keys_b, rc):
     return len(diff)
 
 
-@pytest.mark.parametrize("kind", ["periodic", "open"])
+@pytest.mark.parametrize("kind", ["periodic", "open", "ortho"])
 def test_pair_set_matches_reference_lj_mix(golden, kind):
     from devinproj_b200 import cell_list_pairs
     g = golden(f"lj_mix_{kind}")
@@ -76,7 +76,7 @@ def test_pair_set_digest_nacl4096(golden):
     assert hashlib.sha256(key.tobytes()).hexdigest() == str(g["pairs_dsf_sha"])
 
 
-@pytest.mark.parametrize("kind", ["periodic", "open"])
+@pytest.mark.parametrize("kind", ["periodic", "open", "ortho"])
 def test_lj_fp64_matches_reference(golden, kind):
     from devinproj_b200 import LennardJones
     g = golden(f"lj_mix_{kind}")

@@ -9,7 +9,7 @@ from oracle import accusim_port as port
 from tests._helpers import oracle_state, pair_keys, rel_max
 
 
-@pytest.mark.parametrize("kind", ["periodic", "open"])
+@pytest.mark.parametrize("kind", ["periodic", "open", "ortho"])
 def test_oracle_lj_mix_matches_reference(golden, kind):
     g = golden(f"lj_mix_{kind}")
     st = oracle_state(g)
