@@ -7,6 +7,8 @@ The .npz files it writes are committed; nothing at test time imports the referen
 Each case restates a reference test or example setup (file:line inside the accusim project):
   lj_mix_{periodic,open}  tests/test_forces.py:64-76   300 Ar + 200 Kr, 4 nm box
   lj_mix_ortho            the same mixture in a periodic 4 x 3 x 5.2 nm box (unequal edges)
+  coulomb_ortho           rock salt 10 x 8 x 12 sites, perturbed, in its box of unequal edges: DSF (dense and
+                          cell paths, tests/test_dsf.py:55-61) and Ewald (tests/test_dsf.py:46-52)
   argon864                examples/rahman_argon.py:19-30 geometry at the fcc 6^3 / L=10.229 sigma config
   lj500_skin              tests/test_nose_hoover.py:6-17, 51-60   skin == fresh list along a VV run
   dsf_rocksalt10          tests/test_dsf.py:55-61       DSF dense == cell path
@@ -169,6 +171,23 @@ def dsf_cases():
          rebuilds=skinned._vl.rebuilds, F=f1, U=u1, pos_series=np.array(Ps, dtype=np.float64)[::6])
 
 
+def coulomb_ortho():
+    s = System(3, box=np.array([10.0, 8.0, 12.0]), periodic=True)
+    s.add_species("Na", 1.0, charge=1.0)
+    s.add_species("Cl", 1.0, charge=-1.0)
+    g = np.stack(np.meshgrid(np.arange(10), np.arange(8), np.arange(12), indexing="ij"), -1).reshape(-1, 3)
+    odd = g.sum(1) % 2 == 1
+    s.add("Na", g[~odd].astype(float))
+    s.add("Cl", g[odd].astype(float))
+    rng = np.random.default_rng(11)
+    s.pos = (s.pos + rng.normal(0, 0.2, s.pos.shape)) % s.box
+    fd, ud = DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=10 ** 9).compute(s)
+    fc, uc = DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=1).compute(s)
+    Fe, Ue = Ewald(k=1.0).compute(s)
+    save("coulomb_ortho", **state_arrays(s), rcut=2.5, alpha=2.0 / 2.5, k=1.0, F_dense=fd, U_dense=ud,
+         F_list=fc, U_list=uc, F_ewald=Fe, U_ewald=Ue)
+
+
 def nacl4096():
     n = 16
     mass_g = n ** 3 / 2 * (22.98977 + 35.453) / N_A
@@ -272,6 +291,7 @@ def analysis_cases():
 CASES = {
     "lj_mix": lambda: (lj_mix(True), lj_mix(False)),
     "lj_mix_ortho": lambda: lj_mix(True, box=(4e-9, 3e-9, 5.2e-9), name="lj_mix_ortho"),
+    "coulomb_ortho": coulomb_ortho,
 }
 
 
@@ -284,6 +304,7 @@ if __name__ == "__main__":
     lj_mix(True)
     lj_mix(False)
     CASES["lj_mix_ortho"]()
+    coulomb_ortho()
     argon864()
     lj500_skin()
     dsf_cases()

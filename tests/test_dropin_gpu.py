@@ -167,6 +167,16 @@ def test_dsf_fp64_matches_reference(golden):
     assert rel_max(fc, g["F_list"]) <= TOL and abs(uc - g["U_list"]) <= TOL * abs(g["U_list"])
 
 
+def test_dsf_fp64_matches_reference_in_orthorhombic_box(golden):
+    from devinproj_b200 import DampedShiftedCoulomb
+    g = golden("coulomb_ortho")
+    s = product_system(g)
+    fd, ud = DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=10 ** 9).compute(s)
+    fc, uc = DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=1).compute(s)
+    assert rel_max(fd, g["F_dense"]) <= TOL and abs(ud - g["U_dense"]) <= TOL * abs(g["U_dense"])
+    assert rel_max(fc, g["F_list"]) <= TOL and abs(uc - g["U_list"]) <= TOL * abs(g["U_list"])
+
+
 def test_dsf_exclusions_match_reference(golden):
     from devinproj_b200 import DampedShiftedCoulomb
     g = golden("dsf_exclusions")

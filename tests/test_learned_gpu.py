@@ -11,6 +11,15 @@ from tests.test_dropin_gpu import product_system
 pytestmark = pytest.mark.gpu
 
 
+def test_ewald_matches_reference_in_orthorhombic_box(golden):
+    from devinproj_b200.ewald import Ewald
+    g = golden("coulomb_ortho")
+    s = product_system(g)
+    F, U = Ewald(k=1.0).compute(s)
+    assert rel_max(F, g["F_ewald"]) <= 1e-10
+    assert abs(U - g["U_ewald"]) <= 1e-10 * abs(g["U_ewald"])
+
+
 def test_ewald_matches_reference_on_disordered_melt(golden):
     from devinproj_b200.ewald import Ewald
     g = golden("ewald_melt512")

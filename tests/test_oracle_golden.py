@@ -61,6 +61,18 @@ def test_oracle_dsf_matches_reference(golden):
     assert np.array_equal(fc, g["F_list"]) and uc == g["U_list"]
 
 
+def test_oracle_coulomb_in_orthorhombic_box_matches_reference(golden):
+    """DSF (dense and cell paths) and Ewald in a periodic box of unequal edges, as the reference computes them."""
+    g = golden("coulomb_ortho")
+    st = oracle_state(g)
+    fd, ud = port.DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=10 ** 9).compute(st)
+    fc, uc = port.DampedShiftedCoulomb(rcut=2.5, k=1.0, pairlist_threshold=1).compute(st)
+    assert np.array_equal(fd, g["F_dense"]) and ud == g["U_dense"]
+    assert np.array_equal(fc, g["F_list"]) and uc == g["U_list"]
+    F, U = port.Ewald(k=1.0).compute(st)
+    assert rel_max(F, g["F_ewald"]) < 1e-12 and abs(U - g["U_ewald"]) <= 1e-12 * abs(g["U_ewald"])
+
+
 def test_oracle_dsf_exclusions_match_reference(golden):
     g = golden("dsf_exclusions")
     st = oracle_state(g)
