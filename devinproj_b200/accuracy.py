@@ -8,7 +8,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .units import k_B
+from .units import c_light, k_B
 
 from .units import si
 
@@ -127,9 +127,86 @@ class AccuracyReport:
             tol = max(0.02, 3 * np.sqrt(2 / (s.dim * max(s.n, 1))))
             checks.append(Check("thermostat", PASS if dev <= tol else (WARN if dev <= 0.1 else FAIL), dev,
                                 f"mean T over 2nd half {T_meas:.4g} K vs target {integ.T:.4g} K"))
+        if kind != "Brownian":
+            ts = timescales(sim)
+            if ts:
+                # accusim/accuracy.py:126-133
+                tkind, tmin = min(ts.items(), key=lambda kv: kv[1])
+                ratio = sim.dt / tmin
+                checks.append(Check("timestep vs physics", _grade(ratio, 0.02, 0.1), ratio,
+                                    f"dt / shortest timescale ({tkind}, {tmin:.3g} s) at end of run"))
+        for f in [f for f in sim.forces if type(f).__name__ == "DampedShiftedCoulomb"]:
+            # accusim/accuracy.py:148-161, with the device Ewald (pinned to the reference's)
+            q = s.charges
+            if not (s.periodic and s.dim == 3 and np.any(q)):
+                continue
+            if f.exclude or abs(q.sum()) > 1e-9 * np.sum(np.abs(q)) or s.n > 2000:
+                checks.append(Check("DSF vs Ewald", NA, None, "needs a neutral system, no exclusions, n <= 2000"))
+                continue
+            from .ewald import Ewald
+            F_d = f.compute(s)[0]
+            F_e = Ewald(k=f.k).compute(s)[0]
+            e = float(np.sqrt(np.mean(np.sum((F_d - F_e) ** 2, 1)) / np.mean(np.sum(F_e ** 2, 1))))
+            checks.append(Check("DSF vs Ewald", _grade(e, 5e-2, 2e-1), e,
+                                "RMS force error of the cutoff method vs Ewald, final snapshot (inflated for "
+                                "near-crystalline states)"))
+        # accusim/accuracy.py:176-182
+        beta2 = float(np.max(np.sum(s.vel ** 2, axis=1)) / c_light ** 2) if s.n else 0.0
+        checks.append(Check("relativity", _grade(beta2, 1e-4, 1e-2), beta2,
+                            f"(v/c)^2 of fastest particle: Newtonian error ~ this size (v = {np.sqrt(beta2):.3g} c)"))
         if convergence_duration is not None:
             checks.append(timestep_convergence(sim, convergence_duration))
         return cls(checks)
+
+
+def _closest_approach(s, max_rows=1500):
+    """Smallest distance from the sampled atoms to any other atom (accusim/advisor.py:15-22: every atom for
+    n <= max_rows, else max_rows atoms drawn by default_rng(0)), from the device cell list at a radius that
+    doubles until some pair holds a sampled atom (any closer pair is then inside it too), instead of the
+    reference's dense rows x n distance matrix."""
+    from .forces import cell_list_pairs
+    n = s.n
+    sub = np.arange(n) if n <= max_rows else np.random.default_rng(0).choice(n, max_rows, replace=False)
+    mark = np.zeros(n, dtype=bool)
+    mark[sub] = True
+    extent = s.box if s.box is not None else np.ptp(s.pos, axis=0)
+    extent = np.maximum(np.asarray(extent, dtype=float), 1e-300)
+    R = 2.0 * (float(np.prod(extent)) / n) ** (1.0 / 3.0)
+    diameter = float(np.linalg.norm(extent))
+    while True:
+        i, j = cell_list_pairs(s, R)
+        keep = mark[i] | mark[j]
+        if np.any(keep) or R > 2.0 * diameter:
+            break
+        R *= 2.0
+    if not np.any(keep):
+        return np.inf
+    d = s.pos[j[keep]] - s.pos[i[keep]]
+    if s.periodic:
+        d -= s.box * np.round(d / s.box)
+    return float(np.sqrt(np.min(np.einsum("ij,ij->i", d, d))))
+
+
+def timescales(sim) -> dict:
+    """Shortest characteristic times (s) of the physics on this path (accusim/advisor.py:9-44): the
+    Lennard-Jones time sigma_ii sqrt(m_i / eps_ii) of each interacting species, and the closest approach over
+    the fastest speed."""
+    s = sim.system
+    out = {}
+    if s.n < 2:
+        return out
+    for f in sim.forces:
+        if type(f).__name__ == "LennardJones":
+            eps_t, sig_t = f._tables(s)
+            for i, sp in enumerate(s.species):
+                if eps_t[i, i] > 0:
+                    t = sig_t[i, i] * np.sqrt(sp.mass / eps_t[i, i])
+                    out["Lennard-Jones"] = min(out.get("Lennard-Jones", np.inf), float(t))
+    speed = float(np.max(np.linalg.norm(s.vel, axis=1)))
+    if speed > 0 and any(not f.external for f in sim.forces):
+        eps2 = max([getattr(f, "eps2", 0.0) for f in sim.forces] or [0.0])
+        out["closest approach / speed"] = float(np.sqrt(_closest_approach(s) ** 2 + eps2) / speed)
+    return out
 
 
 def richardson_check(finals, n, order) -> Check:

@@ -7,6 +7,10 @@ The .npz files it writes are committed; nothing at test time imports the referen
 Each case restates a reference test or example setup (file:line inside the accusim project):
   lj_mix_{periodic,open}  tests/test_forces.py:64-76   300 Ar + 200 Kr, 4 nm box
   lj_mix_ortho            the same mixture in a periodic 4 x 3 x 5.2 nm box (unequal edges)
+  report_argon108         accusim/accuracy.py:60-110, 191-221: the accuracy report of a 60-step VelocityVerlet
+                          run of 108 argon atoms, with the dt/2, dt/4 Richardson runs over 0.3 ps
+  report_nacl512          the same for a 512-ion NaCl melt (LJ + DSF, 20 steps of 1 fs, Richardson over 10 fs):
+                          adds the two-species timescales and the DSF vs Ewald row (accusim/accuracy.py:148-161)
   coulomb_ortho           rock salt 10 x 8 x 12 sites, perturbed, in its box of unequal edges: DSF (dense and
                           cell paths, tests/test_dsf.py:55-61) and Ewald (tests/test_dsf.py:46-52)
   argon864                examples/rahman_argon.py:19-30 geometry at the fcc 6^3 / L=10.229 sigma config
@@ -256,6 +260,50 @@ def thermostats108():
          T=120.0, friction=5e12, seed=11, tau=Q(0.2, "ps").value)
 
 
+def report_argon108():
+    m = Q(39.948, "u").value
+    L = (4 * 27 * m / 1374.0) ** (1 / 3)
+    s = System(3, box=L, periodic=True)
+    s.add_species("Ar", m)
+    s.add("Ar", fcc(3, L))
+    s.maxwell_boltzmann(90.0, np.random.default_rng(8))
+    init = state_arrays(s)
+    lj = LennardJones({"Ar": (120 * k_B.value, 3.4e-10)}, cutoff=2.5)
+    sim = Simulation(s, [lj], integrator=VelocityVerlet(), dt=Q(5, "fs"))
+    sim.run(steps=60, record_every=1, positions=False)
+    rep = sim.accuracy_report(convergence_duration=Q(0.3, "ps"))
+    save("report_argon108", **init, eps=120 * k_B.value, sig=3.4e-10, dt=Q(5, "fs").value, steps=60,
+         convergence_duration=Q(0.3, "ps").value,
+         names=np.array([c.name for c in rep.checks]), statuses=np.array([c.status for c in rep.checks]),
+         values=np.array([np.nan if c.value is None else float(c.value) for c in rep.checks]))
+
+
+def report_nacl512():
+    n = 8
+    mass_g = n ** 3 / 2 * (22.98977 + 35.453) / N_A
+    L = (mass_g / 1.55) ** (1 / 3) * 1e-2
+    s = System(3, box=L, periodic=True)
+    s.add_species("Na", Q(22.98977, "u"), charge=Q(1, "e"))
+    s.add_species("Cl", Q(35.453, "u"), charge=Q(-1, "e"))
+    g = np.stack(np.meshgrid(*[np.arange(n)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    odd = g.sum(1) % 2 == 1
+    s.add("Na", (g[~odd] + 0.5) * L / n)
+    s.add("Cl", (g[odd] + 0.5) * L / n)
+    s.maxwell_boltzmann(1300, rng=np.random.default_rng(12))
+    init = state_arrays(s)
+    params = {"Na": (0.544e3 / N_A, 2.35e-10), "Cl": (0.418e3 / N_A, 4.40e-10)}
+    lj = LennardJones(params, cutoff=2.5)
+    dsf = DampedShiftedCoulomb(rcut=10e-10, alpha=Q(0.2, "1/A"))
+    sim = Simulation(s, [lj, dsf], integrator=VelocityVerlet(), dt=Q(1, "fs"))
+    sim.run(steps=20, record_every=1, positions=False)
+    rep = sim.accuracy_report(convergence_duration=Q(10, "fs"))
+    save("report_nacl512", **init, param_names=np.array(["Na", "Cl"]),
+         param_eps=np.array([0.544e3 / N_A, 0.418e3 / N_A]), param_sig=np.array([2.35e-10, 4.40e-10]),
+         rcut=10e-10, alpha=0.2e10, dt=Q(1, "fs").value, steps=20, convergence_duration=Q(10, "fs").value,
+         names=np.array([c.name for c in rep.checks]), statuses=np.array([c.status for c in rep.checks]),
+         values=np.array([np.nan if c.value is None else float(c.value) for c in rep.checks]))
+
+
 def analysis_cases():
     from accusim import analysis
     from accusim import io as aio
@@ -292,6 +340,8 @@ CASES = {
     "lj_mix": lambda: (lj_mix(True), lj_mix(False)),
     "lj_mix_ortho": lambda: lj_mix(True, box=(4e-9, 3e-9, 5.2e-9), name="lj_mix_ortho"),
     "coulomb_ortho": coulomb_ortho,
+    "report_argon108": report_argon108,
+    "report_nacl512": report_nacl512,
 }
 
 
@@ -311,4 +361,6 @@ if __name__ == "__main__":
     nacl4096()
     ewald_melt()
     thermostats108()
+    report_argon108()
+    report_nacl512()
     analysis_cases()

@@ -382,6 +382,37 @@ def test_dropin_thermostats_match_reference(golden, kind):
     assert "thermostat" in rows and (("extended energy" in rows) == (kind == "nh"))
 
 
+@pytest.mark.parametrize("case", ["report_argon108", "report_nacl512"])
+def test_accuracy_report_matches_reference(golden, case):
+    """The accuracy report (accusim/accuracy.py:60-182, 191-221) of a short VelocityVerlet run with the dt/2,
+    dt/4 Richardson runs, through the plug-ins, against the reference's own report: 108 argon atoms (60 steps)
+    and a 512-ion NaCl melt (LJ + DSF, 20 steps: two species' timescales and the DSF vs Ewald row). The same
+    rows and grades; values to 1e-6 relative where they are not round-off (the device FP64 forces differ from
+    NumPy's at round-off and the runs are short)."""
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, Simulation, VelocityVerlet
+    g = golden(case)
+    s = product_system(g)
+    if case == "report_argon108":
+        forces = [LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)]
+    else:
+        params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+        forces = [LennardJones(params, cutoff=2.5), DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"]))]
+    sim = Simulation(s, forces, integrator=VelocityVerlet(), dt=float(g["dt"]))
+    sim.run(steps=int(g["steps"]), record_every=1, positions=False)
+    rep = sim.accuracy_report(convergence_duration=float(g["convergence_duration"]))
+    assert [c.name for c in rep.checks] == [str(x) for x in g["names"]]
+    assert [c.status for c in rep.checks] == [str(x) for x in g["statuses"]]
+    for c, v in zip(rep.checks, g["values"]):
+        if np.isnan(v):
+            assert c.value is None, c.name
+        elif c.name == "momentum":        # round-off of a conserved sum: both far below the PASS grade
+            assert c.value <= 1e-12 and v <= 1e-12
+        elif v == 0.0:
+            assert c.value == 0.0, c.name
+        else:
+            assert abs(c.value - v) <= 1e-6 * abs(v), (c.name, c.value, v)
+
+
 def test_langevin_o_step_is_bit_identical():
     """Given the same velocities, per-atom sigma and normal draws, acs_langevin_ou computes the reference's
     c1 * v + sig * noise exactly (accusim/integrators.py:66-67)."""
