@@ -3,7 +3,7 @@
 Drop-in plug-ins with the reference's interfaces (`LennardJones`, `DampedShiftedCoulomb`,
 `VelocityVerlet`, driven by `Simulation.run`) backed by hand-written CUDA in libaccusim_b200.so.
 """
-from .accuracy import AccuracyReport, calibrate_dt, timestep_convergence
+from .accuracy import AccuracyReport, calibrate_dt, suggest_dt, timescales, timestep_convergence
 from .engine import GpuSimulation
 from .ewald import Ewald
 from .learned import LearnedCorrection
@@ -15,5 +15,5 @@ from .units import k_B, k_e
 
 __all__ = ["AccuracyReport", "Ewald", "GpuSimulation", "LearnedCorrection", "DampedShiftedCoulomb", "Force", "Integrator", "LennardJones", "Simulation",
            "Langevin", "NoseHoover", "Species", "System", "Trajectory", "VelocityVerlet", "VerletList", "calibrate_dt", "cell_list_pairs",
-           "k_B", "k_e", "timestep_convergence"]
+           "k_B", "k_e", "suggest_dt", "timescales", "timestep_convergence"]
 __version__ = "0.1.0"

@@ -227,6 +227,14 @@ def richardson_check(finals, n, order) -> Check:
                  f"est. position error at dt (relative to system size), observed order {p:.1f}/{order}")
 
 
+def suggest_dt(sim, steps_per_timescale: int = 100) -> float:
+    """accusim/advisor.py:51-55: the shortest physical timescale divided by `steps_per_timescale`."""
+    ts = timescales(sim)
+    if not ts:
+        raise ValueError("no timescale found; choose dt manually")
+    return min(ts.values()) / steps_per_timescale
+
+
 def timestep_convergence(sim, duration, start=None) -> Check:
     """Re-run from the initial state at dt, dt/2, dt/4 and estimate the error at dt
     (accusim/accuracy.py:191-221)."""

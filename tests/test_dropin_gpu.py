@@ -411,6 +411,10 @@ def test_accuracy_report_matches_reference(golden, case):
             assert c.value == 0.0, c.name
         else:
             assert abs(c.value - v) <= 1e-6 * abs(v), (c.name, c.value, v)
+    # accusim/advisor.py:51-55 on the same end-of-run state: the shortest timescale / 100
+    from devinproj_b200 import suggest_dt
+    ratio = float(g["values"][list(g["names"]).index("timestep vs physics")])
+    assert suggest_dt(sim) == pytest.approx(float(g["dt"]) / ratio / 100, rel=1e-6)
 
 
 def test_langevin_o_step_is_bit_identical():
