@@ -260,10 +260,8 @@ def calibrate_dt(sim, trial_duration, energy_tol=1e-6, max_halvings=12):
     (accusim/advisor.py:58-79)."""
     if sim.integrator.stochastic or sim.integrator.thermostat or not all(f.conservative for f in sim.forces):
         raise ValueError("calibrate_dt needs conservative, deterministic physics")
-    if sim.dt is None:
-        raise ValueError("set sim.dt to the largest dt to try")
     T = si(trial_duration, "s")
-    dt = sim.dt
+    dt = sim.dt if sim.dt is not None else suggest_dt(sim)
     drift = float("nan")
     for _ in range(max_halvings + 1):
         trial = sim.clone(dt=dt)

@@ -9,6 +9,8 @@ Each case restates a reference test or example setup (file:line inside the accus
   lj_mix_ortho            the same mixture in a periodic 4 x 3 x 5.2 nm box (unequal edges)
   report_argon108         accusim/accuracy.py:60-110, 191-221: the accuracy report of a 60-step VelocityVerlet
                           run of 108 argon atoms, with the dt/2, dt/4 Richardson runs over 0.3 ps
+  calibrate_argon108      accusim/advisor.py:51-79: calibrate_dt from dt = 40 fs (halvings) and from dt unset
+                          (suggest_dt), 108 argon atoms, 0.4 ps trials, energy tolerance 1e-5
   report_nacl512          the same for a 512-ion NaCl melt (LJ + DSF, 20 steps of 1 fs, Richardson over 10 fs):
                           adds the two-species timescales and the DSF vs Ewald row (accusim/accuracy.py:148-161)
   coulomb_ortho           rock salt 10 x 8 x 12 sites, perturbed, in its box of unequal edges: DSF (dense and
@@ -304,6 +306,25 @@ def report_nacl512():
          values=np.array([np.nan if c.value is None else float(c.value) for c in rep.checks]))
 
 
+def calibrate_argon108():
+    from accusim.advisor import calibrate_dt
+    m = Q(39.948, "u").value
+    L = (4 * 27 * m / 1374.0) ** (1 / 3)
+    s = System(3, box=L, periodic=True)
+    s.add_species("Ar", m)
+    s.add("Ar", fcc(3, L))
+    s.maxwell_boltzmann(90.0, np.random.default_rng(21))
+    init = state_arrays(s)
+    out = {}
+    for tag, dt0 in (("from40fs", Q(40, "fs")), ("suggested", None)):
+        lj = LennardJones({"Ar": (120 * k_B.value, 3.4e-10)}, cutoff=2.5)
+        sim = Simulation(s.copy(), [lj], integrator=VelocityVerlet(), dt=dt0)
+        dt, drift = calibrate_dt(sim, Q(0.4, "ps"), energy_tol=1e-5)
+        out[f"{tag}_dt"], out[f"{tag}_drift"] = dt, drift
+    save("calibrate_argon108", **init, eps=120 * k_B.value, sig=3.4e-10, trial=Q(0.4, "ps").value, tol=1e-5,
+         dt0=Q(40, "fs").value, **out)
+
+
 def analysis_cases():
     from accusim import analysis
     from accusim import io as aio
@@ -342,6 +363,7 @@ CASES = {
     "coulomb_ortho": coulomb_ortho,
     "report_argon108": report_argon108,
     "report_nacl512": report_nacl512,
+    "calibrate_argon108": calibrate_argon108,
 }
 
 
@@ -363,4 +385,5 @@ if __name__ == "__main__":
     thermostats108()
     report_argon108()
     report_nacl512()
+    calibrate_argon108()
     analysis_cases()
