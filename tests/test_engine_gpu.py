@@ -269,6 +269,35 @@ def test_batched_replicas_equal_single_runs_bitwise():
     assert batch.status().rebuilds > 3
 
 
+def test_batched_nose_hoover_replicas_equal_single_runs_bitwise():
+    """Nose-Hoover keeps one thermostat per replica (its kinetic-energy sums, xi and eta): replicas of
+    different sizes and dt under Nose-Hoover in one engine advance, thermostat state included, exactly as each
+    would alone, across several graph blocks."""
+    from devinproj_b200 import NoseHoover, configs
+    from devinproj_b200.engine import nose_hoover_thermostat, start_engine
+    th = nose_hoover_thermostat(NoseHoover(120.0, 0.2e-12))
+    systems, dts = [], []
+    for nc, T, dtf in [(4, 0.5, 1.0), (5, 1.0, 0.5), (6, 0.72, 0.25)]:
+        s, lj = configs.lj_fluid(nc, T_star=T, seed=10 + nc)
+        systems.append(s)
+        dts.append(0.005 * configs.AR_TAU * dtf)
+    batch, _, _ = start_engine(systems, [lj], dts, thermo=th)
+    for _ in range(3):
+        batch.run(20, 10, True)
+    bp, bv, _ = batch.get_state()
+    bp, bv, bnh = bp.cpu().numpy(), bv.cpu().numpy(), batch.nh_state()
+    assert np.all(bnh[:, 0] != 0)
+    for k, (s, dt) in enumerate(zip(systems, dts)):
+        eng, _, _ = start_engine([s], [lj], [dt], maxnb=batch.maxnb, tpa=batch.tpa, thermo=th)
+        for _ in range(3):
+            eng.run(20, 10, True)
+        p, v, _ = eng.get_state()
+        sl = slice(batch.offsets[k], batch.offsets[k + 1])
+        assert np.array_equal(p.cpu().numpy(), bp[sl]), k
+        assert np.array_equal(v.cpu().numpy(), bv[sl]), k
+        assert np.array_equal(eng.nh_state()[0], bnh[k]), k
+
+
 def test_engine_rejects_unsupported_setups():
     from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones, System
     s = System(3, box=None)
