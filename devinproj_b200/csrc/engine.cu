@@ -1599,6 +1599,7 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     R.n = q.n;
     R.npad = (q.n + 31) / 32 * 32;
     int64_t ncell = 1;
+    bool small = false;   // list radius >= half a box edge
     for (int d = 0; d < 3; ++d) {
       if (!(q.box[d] > 0.0)) {
         err = ACS_ERR_ARG;
@@ -1614,7 +1615,7 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
       R.cs[d] = q.box[d] / nc;
       R.csf[d] = (float)R.cs[d];
       ncell *= nc;
-      if (q.rlist * 2.0 >= q.box[d]) err = ACS_ERR_UNSUPPORTED;  // minimum image needs rlist < box/2
+      small |= q.rlist * 2.0 >= q.box[d];
     }
     if (err) return;
     R.cellbase = C;
@@ -1628,7 +1629,11 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     NCC += R.ncc;
     R.dt = q.dt;
     R.hdt = 0.5 * q.dt;
-    R.hs2 = q.half_skin * q.half_skin;
+    // A list entry keeps one periodic image per pair. When the list radius reaches half a box edge a pair's
+    // minimum image can change between rebuilds, so such a replica rebuilds its lists every step (half skin 0:
+    // every step flags it): each force evaluation then sees the minimum images of its own positions, as the
+    // reference's per-evaluation re-imaging gives (accusim/forces.py:316-321).
+    R.hs2 = small ? 0.0 : q.half_skin * q.half_skin;
     R.rl2 = q.rlist * q.rlist;
     if (cfg->thermo.kind == 2) {  // accusim/integrators.py:86-92: N_f = dim (n - 1), Q = N_f kT tau^2
       const double nf = 3.0 * (double)std::max(q.n - 1, 1);

@@ -182,7 +182,7 @@ class Engine:
             self.cfg.n_ex_ids = len(ex_start) - 1
         nbytes = L.acs_engine_bytes(C.byref(self.cfg))
         if nbytes == 0:
-            raise ValueError("engine configuration rejected (sizes, list radius >= box/2, or too many replicas)")
+            raise ValueError("engine configuration rejected (sizes, box, time step or too many replicas)")
         self.nbytes = int(nbytes)
         self.mem = torch.empty(self.nbytes + 256, dtype=torch.uint8, device="cuda")
         base = self.mem.data_ptr()

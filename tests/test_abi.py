@@ -84,7 +84,8 @@ def _engine_config(n=864, box_sigma=10.229, tpa=1, maxnb=96, thermo=None):
 
 def test_engine_config_validation_is_host_side():
     """acs_engine_bytes sizes the engine's device block on the host: it is positive for valid configurations
-    and 0 for invalid ones (threads per atom, list radius against the box, thermostat parameters)."""
+    and 0 for invalid ones (threads per atom, box, thermostat parameters); a list radius of half the box or more
+    is valid (such a replica rebuilds its lists every step)."""
     from devinproj_b200 import engine as E
     from devinproj_b200.engine import ENGINE_SIGNATURES
     L = _lib.lib()
@@ -96,12 +97,14 @@ def test_engine_config_validation_is_host_side():
     for tpa in (2, 4, 8, 16, 32):
         c2, k2 = _engine_config(tpa=tpa)
         assert L.acs_engine_bytes(C.byref(c2)) > 0
-    bad = [_engine_config(tpa=3), _engine_config(box_sigma=5.0),   # rlist must stay below box / 2
+    bad = [_engine_config(tpa=3), _engine_config(box_sigma=0.0),
            _engine_config(thermo=E.Thermostat(3, 0, 1.0, 1.0, 0, 0.0)),
            _engine_config(thermo=E.Thermostat(1, 0, 1.0, -1.0, 0, 0.0)),
            _engine_config(thermo=E.Thermostat(2, 0, 1.0, 0.0, 0, 0.0))]
     for c3, k3 in bad:
         assert L.acs_engine_bytes(C.byref(c3)) == 0
+    small, ks = _engine_config(box_sigma=5.0)
+    assert L.acs_engine_bytes(C.byref(small)) > 0
     good = [E.Thermostat(1, 0, 0.997, 0.05, 7, 0.0), E.Thermostat(2, 0, 0.997, 0.0, 0, 2.0)]
     for th in good:
         c4, k4 = _engine_config(thermo=th)

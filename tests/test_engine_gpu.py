@@ -163,6 +163,36 @@ def test_engine_orthorhombic_boxes(nz, tpa):
         assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
 
 
+def test_engine_box_smaller_than_twice_the_list_radius(golden):
+    """108 argon atoms (a displaced fcc lattice) in a 17.3 A box, list radius 9.5 A: a pair's minimum image can
+    change between rebuilds, so the engine rebuilds this replica's lists every step; forces against the FP64
+    plug-in at the start and after 100 steps, one rebuild per step, and the energy drift of the 100 steps no
+    more than 10x the reference's over its 60-step run of the undisplaced lattice."""
+    from devinproj_b200 import GpuSimulation, LennardJones
+    from devinproj_b200.accuracy import energy_drift
+    g = golden("report_argon108")
+    s = product_system(g)
+    assert 2 * 2.8 * float(g["sig"]) > s.box[0]
+    # the fcc lattice's forces vanish by symmetry: displace every atom by a seeded 0.05 sigma first
+    s.pos = (s.pos + np.random.default_rng(2).normal(0, 0.05 * float(g["sig"]), s.pos.shape)) % s.box
+    lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
+    sim = GpuSimulation(s, [lj], dt=float(g["dt"]))
+    rb0 = sim.rebuilds
+    tr = None
+    for stage in ("start", "after 100 steps"):
+        if stage != "start":
+            tr = sim.run(steps=100, record_every=1, positions=False)
+        F64, U64 = lj.compute(s)
+        e = rms_rel(sim.force, F64)
+        print(f"argon108 small box, {stage}: force RMS rel error {e:.2e}")
+        assert e <= 1e-5, stage
+        assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
+    assert sim.rebuilds - rb0 >= 100
+    ref = float(g["values"][list(g["names"]).index("energy")])
+    print(f"energy drift {energy_drift(tr):.2e} (reference, 60 steps: {ref:.2e})")
+    assert energy_drift(tr) <= 10 * ref
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
@@ -305,11 +335,12 @@ def test_engine_rejects_unsupported_setups():
     s.add("Ar", np.random.default_rng(0).uniform(0, 3e-9, (50, 3)))
     with pytest.raises(ValueError):
         GpuSimulation(s, [LennardJones({"Ar": (1.6e-21, 3.4e-10)})], dt=1e-15)
-    s2 = System(3, box=4e-10, periodic=True)   # list radius >= box/2
+    s2 = System(3, box=4e-9, periodic=True)    # two LennardJones forces
     s2.add_species("Ar", 6.6e-26)
-    s2.add("Ar", [[0, 0, 0], [2e-10, 0, 0]])
+    s2.add("Ar", [[0, 0, 0], [4e-10, 0, 0]])
     with pytest.raises(ValueError):
-        GpuSimulation(s2, [LennardJones({"Ar": (1.6e-21, 3.4e-10)})], dt=1e-15)
+        GpuSimulation(s2, [LennardJones({"Ar": (1.6e-21, 3.4e-10)}), LennardJones({"Ar": (1.0e-21, 3.0e-10)})],
+                      dt=1e-15)
     s3 = System(3, box=4e-9, periodic=True)
     s3.add_species("Na", 3.8e-26, charge=1.6e-19)
     s3.add("Na", [[0, 0, 0], [2e-10, 0, 0]])

@@ -114,9 +114,10 @@ def test_full_size_ensemble_forces_momentum_and_replica_independence():
 def test_calibrate_dt_matches_reference(golden):
     """accusim/advisor.py:51-79 against the reference's own runs (108 argon atoms, 0.4 ps trials, tolerance
     1e-5): from dt = 40 fs the plug-in halves to the reference's dt, with its drift; with dt unset it starts
-    from suggest_dt, as the reference does. (The batched engine form needs a list radius below half the box,
-    which this 17 A box does not give; the ensemble tests above cover it on larger boxes.)"""
+    from suggest_dt, as the reference does; the batched engine form reaches the same dt (in this 17 A box the
+    list radius exceeds half the box, so the engine rebuilds its lists every step)."""
     from devinproj_b200 import LennardJones, Simulation, VelocityVerlet, calibrate_dt
+    from devinproj_b200.ensemble import calibrate_dt_ensemble
     from tests.test_dropin_gpu import product_system
     g = golden("calibrate_argon108")
     lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
@@ -126,3 +127,6 @@ def test_calibrate_dt_matches_reference(golden):
         assert dt == pytest.approx(float(g[f"{tag}_dt"]), rel=1e-12), tag
         assert drift == pytest.approx(float(g[f"{tag}_drift"]), rel=1e-6), tag
         assert sim.dt == dt
+    d_b, _ = calibrate_dt_ensemble(product_system(g), [lj], float(g["dt0"]), float(g["trial"]),
+                                   energy_tol=float(g["tol"]))
+    assert d_b == pytest.approx(float(g["from40fs_dt"]), rel=1e-12)
