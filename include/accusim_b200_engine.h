@@ -24,7 +24,7 @@ typedef struct acs_replica {
   int32_t pad;
   double box[3];      /* periodic box edges */
   double dt;          /* time step */
-  double rlist;       /* neighbour-list radius = largest cutoff + skin (must be < box/2) */
+  double rlist;       /* neighbour-list radius = largest cutoff + skin (>= half a box edge: lists rebuilt every step) */
   double half_skin;   /* rebuild once an atom has moved this far since the last build */
 } acs_replica;
 
