@@ -186,6 +186,27 @@ def reference_arm(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def bind_to_gpu_local_cores(local):
+    """Run this process on the cores NVML reports as closest to its GPU, so that the pinned host buffers of the
+    end-to-end leg (first touch) sit on the GPU's NUMA node. Affects this process only; returns the number of
+    cores, or None when NVML cannot tell."""
+    try:
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, ((os.cpu_count() or 64) + 63) // 64)
+        cpus = {64 * w + b for w, word in enumerate(words) for b in range(64) if (int(word) >> b) & 1}
+        cpus &= set(os.sched_getaffinity(0))
+        if not cpus:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return len(cpus)
+    except Exception:
+        return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,6 +248,7 @@ def main():
     from datetime import timedelta
 
     torch.cuda.set_device(local)
+    host_cores = bind_to_gpu_local_cores(local) if not args.profile else None
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
@@ -401,7 +423,8 @@ def main():
         "clocks": clocks,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n + 64,
                 "steps": args.e2e_steps, "path": "pinned host pos/vel -> acs_engine_load_state -> 1 step graph -> "
-                                                  "acs_engine_get_state -> pinned host + energy record"},
+                                                  "acs_engine_get_state -> pinned host + energy record",
+                "host_cores": host_cores},
         "gpu_launches": launches,
         "wall_s_timed": wall,
     }
