@@ -193,6 +193,26 @@ def test_engine_box_smaller_than_twice_the_list_radius(golden):
     assert energy_drift(tr) <= 10 * ref
 
 
+def test_gpu_simulation_report_matches_reference_rows(golden):
+    """GpuSimulation's accuracy report (device run, batched FP32c Richardson runs) on the 512-ion NaCl melt of
+    the reference's own report: the same rows; energy, momentum and relativity graded as the reference grades
+    them; the timescale and DSF-vs-Ewald values to 1e-3 (the FP32c state differs from the FP64 one at ~1e-7)."""
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones
+    g = golden("report_nacl512")
+    s = product_system(g)
+    params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+    forces = [LennardJones(params, cutoff=2.5), DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"]))]
+    sim = GpuSimulation(s, forces, dt=float(g["dt"]))
+    sim.run(steps=int(g["steps"]), record_every=1, positions=False)
+    rep = {c.name: c for c in sim.accuracy_report(convergence_duration=float(g["convergence_duration"])).checks}
+    ref = {str(n): (str(st), float(v)) for n, st, v in zip(g["names"], g["statuses"], g["values"])}
+    assert list(rep) == list(ref)
+    for name in ("energy", "momentum", "relativity", "mass-energy", "charge"):
+        assert rep[name].status == ref[name][0], name
+    for name in ("timestep vs physics", "DSF vs Ewald", "relativity"):
+        assert rep[name].value == pytest.approx(ref[name][1], rel=1e-3), name
+
+
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
