@@ -310,7 +310,8 @@ __device__ __forceinline__ void pair_term(const FFDev& ff, const PairK& c1, int 
     const float ar = ff.dsf_a * rr;
     const float ex = __expf(-ar * ar);
     const float er = erfc_as(ar, ex);
-    const float cd = k.qqk * ((er * ir * ir + ff.dsf_c * ex * ir) - ff.dsf_fshift) * ir;
+    // (erfc(ar)/r^2 + c exp(-(ar)^2)/r - fshift)/r, nested as ((erfc/r + c exp) / r - fshift) / r
+    const float cd = k.qqk * (fmaf(fmaf(er, ir, ff.dsf_c * ex), ir, -ff.dsf_fshift) * ir);
     coef -= ind ? cd : 0.f;
     if (REC && ind) kahan_add(eu, ce, k.qqk * (er * ir - ff.dsf_erc_rc + ff.dsf_fshift * (rr - ff.dsf_rc)));
   }
