@@ -265,7 +265,7 @@ struct PairK {
 template <bool ONE>
 __device__ __forceinline__ PairK pair_consts(const FFDev& ff, int p, const PairK& c1) {
   if (ONE) return c1;
-  PairK k;
+  PairK k{};
   k.a = ff.lj_a[p];
   k.b = ff.lj_b[p];
   k.c = ff.lj_c[p];
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
   const uint32_t jm = DSF ? E.jmask : kIdxMask, exb = DSF ? E.ex_bit : 0u;
   const int G = E.G, tpa = E.tpa;
   const int sub_i = lane % G, phase = lane / G;
-  PairK c1;
+  PairK c1{};   // single-species constants (the species-pair kernels read the tables instead)
   c1.eps4 = ff.lj_eps4[0];
   c1.eps24 = ff.lj_eps24[0];
   c1.sig2 = ff.lj_sig2[0];
