@@ -1,5 +1,6 @@
 """Launch-shape autotuner for the engine: threads per atom in the pair kernel (1..32, which also fixes the
-neighbour-list layout) and the step-kernel grid (one thread per slot, or a persistent grid of k blocks per SM).
+neighbour-list layout). The step kernel's grid stays one thread per slot (`grid_mult` 0); a grid of k blocks
+per SM that loops over the slots (`grid_mult` k) is accepted by the engine but not searched.
 
 `tune()` builds the engine for each candidate on the caller's own replicas, times a short eager run with
 CUDA events around every kernel (`acs_engine_run_timed`), and keeps the fastest step + list-maintenance
