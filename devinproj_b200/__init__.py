@@ -1,19 +1,21 @@
-"""accusim_b200: B200-native (sm_100a) short-range force-and-step path of accusim.
+"""devinproj_b200: B200-native (sm_100a) short-range force-and-step path for accusim.
 
-Drop-in plug-ins with the reference's interfaces (`LennardJones`, `DampedShiftedCoulomb`,
-`VelocityVerlet`, driven by `Simulation.run`) backed by hand-written CUDA in libaccusim_b200.so.
+GPU plug-ins that subclass accusim's own classes (`LennardJones`, `DampedShiftedCoulomb`, `VelocityVerlet`,
+`Langevin`, `NoseHoover`, `Ewald`) and run inside accusim's `Simulation.run`; `GpuSystem`, an accusim `System`
+whose state stays on the GPU; and `GpuSimulation`, the device-resident engine (FP32-compensated pairs, FP64
+state, CUDA-graph step loops, batched replicas). All compute is hand-written CUDA in libaccusim_b200.so.
 """
-from .accuracy import AccuracyReport, calibrate_dt, suggest_dt, timescales, timestep_convergence
+from . import _accusim  # noqa: F401  (accusim, the host framework)
+from .analysis import rdf
 from .engine import GpuSimulation
+from .ensemble import ReplicaEnsemble, calibrate_dt_ensemble, richardson_ensemble
 from .ewald import Ewald
+from .forces import DampedShiftedCoulomb, LennardJones, VerletList, cell_list_pairs
+from .integrators import Langevin, NoseHoover, VelocityVerlet
 from .learned import LearnedCorrection
-from .forces import DampedShiftedCoulomb, Force, LennardJones, VerletList, cell_list_pairs
-from .integrators import Integrator, Langevin, NoseHoover, VelocityVerlet
-from .simulation import Simulation, Trajectory
-from .system import Species, System
-from .units import k_B, k_e
+from .state import GpuSystem
 
-__all__ = ["AccuracyReport", "Ewald", "GpuSimulation", "LearnedCorrection", "DampedShiftedCoulomb", "Force", "Integrator", "LennardJones", "Simulation",
-           "Langevin", "NoseHoover", "Species", "System", "Trajectory", "VelocityVerlet", "VerletList", "calibrate_dt", "cell_list_pairs",
-           "k_B", "k_e", "suggest_dt", "timescales", "timestep_convergence"]
-__version__ = "0.1.0"
+__all__ = ["DampedShiftedCoulomb", "Ewald", "GpuSimulation", "GpuSystem", "Langevin", "LearnedCorrection",
+           "LennardJones", "NoseHoover", "ReplicaEnsemble", "VelocityVerlet", "VerletList", "calibrate_dt_ensemble",
+           "cell_list_pairs", "rdf", "richardson_ensemble"]
+__version__ = "0.2.0"

@@ -1,10 +1,10 @@
-"""Observables from a System or a Trajectory: accusim/analysis.py:7-43 (`rdf`, `msd`).
+"""`rdf` (accusim/analysis.py:7-24) with the pair-distance histogram on the GPU.
 
-`rdf` counts pair distances on the GPU (acs_rdf_hist: cell list at radius rmax, the reference's FP64
-minimum image and NumPy's uniform-bin histogram rule), so its counts equal the reference's O(n^2) NumPy
-histogram while needing O(n) memory; the ideal-gas normalisation is the reference's NumPy expression.
-`msd` is the reference's unwrapping of recorded frames (host NumPy; it reads only `t` and `positions`, so
-it works on trajectories of `Simulation` and `GpuSimulation` alike).
+acs_rdf_hist counts pair distances over a cell list at radius rmax with the reference's FP64 minimum image and
+NumPy's uniform-bin histogram rule, so its counts equal the reference's O(n^2) NumPy histogram while needing
+O(n) memory; the ideal-gas normalisation is the reference's NumPy expression. accusim's own `msd` and trajectory
+files (accusim/analysis.py:27-43, accusim/io.py) work unchanged on `GpuSimulation` trajectories, which are
+accusim `Trajectory` objects.
 """
 from __future__ import annotations
 
@@ -47,21 +47,3 @@ def rdf(system, rmax, bins=100, species=None):
     shell = 4 / 3 * np.pi * (edges[1:] ** 3 - edges[:-1] ** 3)
     ideal = shell * n * (n - 1) / 2 / V
     return 0.5 * (edges[1:] + edges[:-1]), hist / ideal
-
-
-def msd(trajectory, box=None):
-    """Mean squared displacement vs time from recorded positions (fixed particle set).
-
-    With a periodic `box`, frames are unwrapped by minimum-image steps, so frames must be recorded often
-    enough that no particle moves half a box between them."""
-    t = np.asarray(trajectory.t)
-    frames = trajectory.positions
-    disp = np.zeros_like(frames[0])
-    out = [0.0]
-    for a, b in zip(frames[:-1], frames[1:]):
-        step = b - a
-        if box is not None:
-            step -= box * np.round(step / box)
-        disp = disp + step
-        out.append(float(np.mean(np.sum(disp ** 2, axis=1))))
-    return t - t[0], np.array(out)

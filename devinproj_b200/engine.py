@@ -18,6 +18,8 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._accusim import forces as _af
+from ._accusim import integrators as _ai
 from .device import require_cuda, stream_handle, to_dev
 from .units import N_A, amu, e_charge, k_B, k_e
 
@@ -54,7 +56,7 @@ class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
                 ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
                 ("thermo", Thermostat), ("ex_start", C.POINTER(C.c_int32)), ("ex_ids", C.POINTER(C.c_int32)),
-                ("n_ex_ids", C.c_int32), ("pad2", C.c_int32)]
+                ("n_ex_ids", C.c_int32), ("pad2", C.c_int32), ("barrier_wait_limit", C.c_int64)]
 
 
 def langevin_thermostat(integrator, seed):
@@ -90,6 +92,7 @@ ENGINE_SIGNATURES = {
     "acs_engine_launch_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "acs_engine_load_state": (C.c_int, [P, P, P, P]),
     "acs_engine_count_pairs": (C.c_int, [P, P, P]),
+    "acs_engine_dump_lists": (C.c_int, [P, P, C.c_longlong, P, P, P]),
     "acs_engine_run_timed": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(C.c_float), P]),
     "acs_engine_phase_times": (C.c_int, [P, P, C.c_int]),
     "acs_engine_set_correction": (C.c_int, [P, P, P, P, P, P, P, C.c_float, P, P, P, P, C.c_int]),
@@ -117,8 +120,8 @@ def forcefield_from(forces, species) -> tuple[ForceField, float, float]:
         ff.mass[a] = sp.mass / MASS
         ff.q[a] = sp.charge / CHARGE
     radii = []   # (cutoff_max, list radius) per force, SI
-    lj = [f for f in forces if type(f).__name__ == "LennardJones"]
-    dsf = [f for f in forces if type(f).__name__ == "DampedShiftedCoulomb"]
+    lj = [f for f in forces if isinstance(f, _af.LennardJones)]
+    dsf = [f for f in forces if isinstance(f, _af.DampedShiftedCoulomb)]
     if len(lj) + len(dsf) != len(forces) or len(lj) > 1 or len(dsf) > 1 or not forces:
         raise ValueError("the engine runs one LennardJones and/or one DampedShiftedCoulomb force")
     if lj:
@@ -155,7 +158,7 @@ class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
     def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
-                 thermo=None, exclusions=None):
+                 thermo=None, exclusions=None, barrier_wait_limit: int = 0):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -174,6 +177,7 @@ class Engine:
         self.tpa = int(tpa)
         self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff,
                                 thermo if thermo is not None else Thermostat())
+        self.cfg.barrier_wait_limit = int(barrier_wait_limit)
         self._ex = exclusions   # (ex_start, ex_ids) int32 arrays, kept alive with the config
         if exclusions is not None:
             ex_start, ex_ids = exclusions
@@ -222,6 +226,22 @@ class Engine:
         _lib.check(self.L.acs_engine_count_pairs(self.h, out.data_ptr(), stream_handle()), "acs_engine_count_pairs")
         a, b = out.cpu().numpy()
         return int(a) // 2, int(b) // 2
+
+    def list_entries(self):
+        """The neighbour lists as they stand: (keys, positions) with keys an int64 device tensor of directed
+        entries 2 (i n + j) + excluded over caller indices (sorted), and the FP64 positions (engine units,
+        caller order) of the last rebuild, which the lists were built from."""
+        n = int(self.offsets[-1])
+        _, total = self.neighbor_stats()
+        keys = torch.empty(max(total, 1), dtype=torch.int64, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        pos = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        _lib.check(self.L.acs_engine_dump_lists(self.h, keys.data_ptr(), int(keys.numel()), cnt.data_ptr(),
+                                                pos.data_ptr(), stream_handle()), "acs_engine_dump_lists")
+        m = int(cnt.item())
+        if m != total:
+            raise RuntimeError(f"list dump counted {m} entries, the lists hold {total}")
+        return torch.sort(keys[:m]).values, pos
 
     def get_state(self):
         n = int(self.offsets[-1])
@@ -362,7 +382,7 @@ def dsf_exclusions(forces, systems):
     index, both directions, ids mapped to indices through `system.ids` as accusim/forces.py:418-419 does
     (pairs with an id not in the system are dropped); None without exclusions. The engine applies one table
     to every replica, so the replicas must number their atoms alike."""
-    dsf = [f for f in forces if type(f).__name__ == "DampedShiftedCoulomb"]
+    dsf = [f for f in forces if isinstance(f, _af.DampedShiftedCoulomb)]
     if not dsf or not dsf[0].exclude:
         return None
     ids = np.asarray(systems[0].ids)
@@ -382,7 +402,7 @@ def dsf_exclusions(forces, systems):
 
 
 def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None,
-                 exclusions=None):
+                 exclusions=None, barrier_wait_limit=0):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -395,7 +415,7 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
         cells = sum(int(np.prod([max(1, int(bx // r["rlist"])) for bx in r["box"]])) for r in reps)
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3, cells)
     return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
-                   exclusions=exclusions), rlist, half_skin)
+                   exclusions=exclusions, barrier_wait_limit=barrier_wait_limit), rlist, half_skin)
 
 
 def _upload_state(engine, systems):
@@ -450,13 +470,16 @@ class GpuSimulation:
 
     def __init__(self, system, forces=(), reactions=(), integrator=None, dt=None, seed=None, maxnb=None,
                  rec_cap=256, grid_mult=0, tpa=None, correction=None, validate_every=500, correction_stride=1):
+        from ._accusim import simulation as _asim
         from .integrators import VelocityVerlet
-        from .simulation import Trajectory
         from .units import si
+        Trajectory = _asim.Trajectory
         if reactions:
             raise NotImplementedError("reactions are not part of the accusim_b200 force-and-step path")
-        kind = type(integrator).__name__ if integrator is not None else "VelocityVerlet"
-        if kind not in ("VelocityVerlet", "Langevin", "NoseHoover"):
+        kind = ("VelocityVerlet" if integrator is None or type(integrator) in (_ai.VelocityVerlet, VelocityVerlet)
+                else "Langevin" if isinstance(integrator, _ai.Langevin)
+                else "NoseHoover" if isinstance(integrator, _ai.NoseHoover) else None)
+        if kind is None:
             raise ValueError("GpuSimulation integrates with VelocityVerlet, Langevin (BAOAB) or NoseHoover")
         thermo = (langevin_thermostat(integrator, seed) if kind == "Langevin"
                   else nose_hoover_thermostat(integrator) if kind == "NoseHoover" else None)
@@ -518,7 +541,7 @@ class GpuSimulation:
         """Check the corrected electrostatic forces against the device Ewald on the current state; switch the
         correction off (fallback to plain DSF) unless it improves on DSF. Returns (err_dsf, err_corrected)."""
         from .ewald import Ewald
-        dsf = [f for f in self.forces if type(f).__name__ == "DampedShiftedCoulomb"][0]
+        dsf = [f for f in self.forces if isinstance(f, _af.DampedShiftedCoulomb)][0]
         Fd, _ = dsf.compute(self.system)
         Fe, _ = Ewald(k=dsf.k).compute(self.system)
         e0, e1, on = self.correction.validate(self.system, Fd, Fe)
@@ -662,8 +685,15 @@ class GpuSimulation:
         return sim
 
     def accuracy_report(self, convergence_duration=None):
-        from .accuracy import AccuracyReport
-        return AccuracyReport.build(self, convergence_duration)
+        """accusim's own AccuracyReport (accusim/accuracy.py:59-188) of this run. The timestep-error row, when
+        asked for, comes from the dt, dt/2, dt/4 runs advanced together in one batched engine and graded by
+        accusim's `timestep_convergence`."""
+        from ._accusim import accuracy as _acc
+        from .ensemble import timestep_check
+        rep = _acc.AccuracyReport.build(self, None)
+        if convergence_duration is not None:
+            rep.checks.append(timestep_check(self, convergence_duration))
+        return rep
 
 
 class _InitialState:

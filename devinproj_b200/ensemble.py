@@ -10,19 +10,42 @@ blocks (`set_active`).
 from __future__ import annotations
 
 import math
+from types import SimpleNamespace
 
 import numpy as np
 
-from .accuracy import Check, _grade, richardson_check
+from ._accusim import accuracy as _acc
 from .engine import ENERGY, LEN, MASS, VEL, start_engine
 from .units import si
 
 
 def drift_of(KE, PE):
-    """Report metric max|E - E0| / max(|E0|, max|KE|, max|PE|) (accusim/accuracy.py:70-76)."""
+    """The energy-drift metric accusim grades and calibrates dt on, max|E - E0| / max(|E0|, max|KE|, max|PE|)
+    (accusim/accuracy.py:70-76, accusim/advisor.py:72-74), of one replica's recorded energies."""
     E = np.asarray(KE) + np.asarray(PE)
     scale = max(abs(E[0]), np.max(np.abs(KE)), np.max(np.abs(PE)), 1e-300)
     return float(np.max(np.abs(E - E[0])) / scale)
+
+
+class _FinishedRuns:
+    """A start state whose runs at dt, dt/2 and dt/4 were already made on the device (in one batched engine):
+    `clone(dt)` hands back the finished run with that time step and its `run` does nothing. Given as `start`
+    to accusim's own `timestep_convergence` (accusim/accuracy.py:191-221), it lets the reference compute the
+    observed order and the Richardson estimate from the batched final positions."""
+
+    def __init__(self, finals):
+        self._finals = finals   # {dt: final positions}
+
+    def clone(self, dt=None):
+        return SimpleNamespace(system=SimpleNamespace(pos=self._finals[dt]), run=lambda **kw: None)
+
+
+def richardson_check(finals, dt, duration, integrator):
+    """accusim's `timestep_convergence` check for a trajectory whose dt, dt/2, dt/4 final positions are
+    `finals` (the three runs advanced together on the device)."""
+    view = SimpleNamespace(dt=dt, integrator=integrator, reactions=None)
+    start = _FinishedRuns({dt / k: f for k, f in zip((1, 2, 4), finals)})
+    return _acc.timestep_convergence(view, duration, start=start)
 
 
 class ReplicaEnsemble:
@@ -102,10 +125,11 @@ class ReplicaEnsemble:
         return drift_of(ke, pe)
 
 
-def richardson_ensemble(systems, forces, dts, duration, order=2, tpa=None):
+def richardson_ensemble(systems, forces, dts, duration, integrator=None, tpa=None):
     """Richardson timestep error for each (system, dt) at once: 3 trajectories per input at dt, dt/2, dt/4
     over the same duration (n, 2n, 4n steps), all in one engine (accusim/accuracy.py:191-221).
-    Returns one `Check` per input, computed with the reference's formulas."""
+    Returns one accusim `Check` per input (computed by accusim's `timestep_convergence` from the finals) and
+    the ensemble."""
     T = float(si(duration, "s"))
     triples, tdts, ns = [], [], []
     for s, dt in zip(systems, dts):
@@ -126,7 +150,11 @@ def richardson_ensemble(systems, forces, dts, duration, order=2, tpa=None):
         ens.run(step, record_every=0)
         remaining[act] -= step
     finals = [p for p, _ in ens.state()]
-    return [richardson_check(finals[3 * q: 3 * q + 3], ns[q], order) for q in range(len(systems))], ens
+    if integrator is None:
+        from .integrators import VelocityVerlet
+        integrator = VelocityVerlet()
+    return [richardson_check(finals[3 * q: 3 * q + 3], dts[q], duration, integrator)
+            for q in range(len(systems))], ens
 
 
 def calibrate_dt_ensemble(system, forces, dt, trial_duration, energy_tol=1e-6, max_halvings=12, per_batch=3,
@@ -160,12 +188,14 @@ def calibrate_dt_ensemble(system, forces, dt, trial_duration, energy_tol=1e-6, m
 
 
 def timestep_check(sim, duration, tpa=None):
-    """`timestep_convergence` (accusim/accuracy.py:191-221) for one simulation, its three runs batched."""
+    """`timestep_convergence` (accusim/accuracy.py:191-221) for one simulation from its initial state, the three
+    runs batched in one engine."""
+    if sim.integrator.stochastic or sim.reactions:
+        return _acc.timestep_convergence(sim, duration)
     base = getattr(sim, "_initial", None)
     system = base.system if base is not None else sim.system
-    checks, _ = richardson_ensemble([system], sim.forces, [sim.dt], duration, order=sim.integrator.order, tpa=tpa)
+    checks, _ = richardson_ensemble([system], sim.forces, [sim.dt], duration, integrator=sim.integrator, tpa=tpa)
     return checks[0]
 
 
-__all__ = ["ReplicaEnsemble", "richardson_ensemble", "calibrate_dt_ensemble", "timestep_check", "drift_of",
-           "Check", "_grade"]
+__all__ = ["ReplicaEnsemble", "richardson_ensemble", "calibrate_dt_ensemble", "timestep_check", "drift_of"]

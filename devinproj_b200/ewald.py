@@ -1,8 +1,9 @@
-"""Ewald summation on the device, with the interface of accusim's `Ewald` (accusim/forces.py:333-388).
+"""accusim's `Ewald` (accusim/forces.py:333-388) evaluated on the device.
 
-Exact periodic electrostatics for a neutral 3-D periodic system: real-space erfc sum over minimum-image
-pairs inside rcut, reciprocal sum over the k-vectors |n| <= kmax (built on the host exactly as the
-reference builds them), self term. Defaults: rcut = L_min / 2, alpha = 4 / rcut, kmax = 12. FP64.
+Exact periodic electrostatics for a neutral 3-D periodic system: real-space erfc sum over minimum-image pairs
+inside rcut, reciprocal sum over the k-vectors |n| <= kmax, self term, in FP64. The class subclasses accusim's:
+the constructor, the defaults (rcut = L_min / 2, alpha = 4 / rcut, kmax = 12) and the k-vector set and weights
+(`_kvectors`) are accusim's own; the real-space and reciprocal sums run as CUDA kernels.
 """
 from __future__ import annotations
 
@@ -10,9 +11,8 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._accusim import forces as _af
 from .device import Workspace, require_cuda, stream_handle, to_dev
-from .forces import Force
-from .units import k_e, si
 
 _lib.SIGNATURES.update({
     "acs_ewald_work_bytes": (_lib.SZ, [_lib.I64, _lib.I32]),
@@ -35,31 +35,19 @@ def _bind():
     return L
 
 
-class Ewald(Force):
-    """Exact periodic electrostatics by Ewald summation (3D orthorhombic box, neutral system)."""
+class Ewald(_af.Ewald):
+    """Exact periodic electrostatics by Ewald summation (3D orthorhombic box, neutral system), on the GPU."""
 
-    def __init__(self, k=k_e, alpha=None, rcut=None, kmax=12):
-        self.k = si(k, "J*m/C^2")
-        self.alpha = None if alpha is None else si(alpha, "1/m")
-        self.rcut = None if rcut is None else si(rcut, "m")
-        self.kmax = kmax
-        self._kcache = None
-        self._ws = Workspace()
-
-    def _kvectors(self, box, alpha):
-        """accusim/forces.py:347-357: |n| <= kmax sphere without n = 0, k = 2 pi n / box,
-        w = exp(-k^2 / (4 alpha^2)) / k^2."""
+    def _device_kvectors(self, box, alpha):
+        """accusim's k-vectors and weights for this box and alpha, as device tensors (cached)."""
+        kv, w = self._kvectors(box, alpha)
         key = (tuple(box), alpha, self.kmax)
-        if self._kcache is None or self._kcache[0] != key:
-            n = np.arange(-self.kmax, self.kmax + 1)
-            N = np.stack(np.meshgrid(n, n, n, indexing="ij"), -1).reshape(-1, 3)
-            N = N[np.sum(N ** 2, axis=1) <= self.kmax ** 2]
-            N = N[np.any(N != 0, axis=1)]
-            kv = 2 * np.pi * N / box
-            k2 = np.sum(kv ** 2, axis=1)
-            w = np.exp(-k2 / (4 * alpha ** 2)) / k2
-            self._kcache = (key, to_dev(np.ascontiguousarray(kv)), to_dev(np.ascontiguousarray(w)), len(w))
-        return self._kcache[1], self._kcache[2], self._kcache[3]
+        cached = getattr(self, "_dev_k", None)
+        if cached is None or cached[0] != key:
+            cached = (key, to_dev(np.ascontiguousarray(kv, dtype=np.float64)),
+                      to_dev(np.ascontiguousarray(w, dtype=np.float64)), len(w))
+            self._dev_k = cached
+        return cached[1], cached[2], cached[3]
 
     def compute_device(self, s, pos_d, q):
         if s.dim != 3 or not s.periodic:
@@ -70,10 +58,12 @@ class Ewald(Force):
         box = np.ascontiguousarray(s.box, dtype=np.float64)
         rcut = self.rcut or 0.5 * float(np.min(box))
         a = self.alpha or 4.0 / rcut
-        kv, w, K = self._kvectors(box, a)
+        kv, w, K = self._device_kvectors(box, a)
         n = s.n
         F = torch.empty((n, 3), dtype=torch.float64, device="cuda")
         e3 = torch.zeros(3, dtype=torch.float64, device="cuda")
+        if getattr(self, "_ws", None) is None:
+            self._ws = Workspace()
         ws = self._ws.get(L.acs_ewald_work_bytes(n, K))
         q_d = to_dev(q.astype(np.float64))   # held until the launch: a freed tensor's memory is handed out again
         _lib.check(L.acs_ewald_fp64(pos_d.data_ptr(), q_d.data_ptr(), n, box.ctypes.data,
@@ -93,5 +83,5 @@ class Ewald(Force):
         if abs(q.sum()) > 1e-9 * np.sum(np.abs(q)):   # the reference's order: checked before any work
             raise ValueError("Ewald summation here requires a charge-neutral system")
         require_cuda()
-        F, U = self.compute_device(s, to_dev(s.pos), q)
+        F, U = self.compute_device(s, to_dev(np.asarray(s.pos, dtype=np.float64)), q)
         return F.cpu().numpy(), float(U)

@@ -1,10 +1,12 @@
-"""GPU drop-ins for accusim's short-range forces: `LennardJones`, `DampedShiftedCoulomb` and the
-`VerletList` they share (accusim/forces.py:78-175, :391-452).
+"""GPU drop-ins for accusim's short-range forces: `LennardJones`, `DampedShiftedCoulomb` and the `VerletList` they
+share (accusim/forces.py:78-175, :391-452).
 
-Same constructor arguments, attributes and `compute(system) -> (F[n, 3] float64 N, U float J)` contract as
-the reference; the pair search and pair loops run as FP64 CUDA kernels in libaccusim_b200.so. Systems
-may be this package's `System` or the reference's; only `pos`, `sp`, `ids`, `box`, `periodic`,
-`species` and `n` are read.
+The classes subclass accusim's own: constructor arguments, attributes (`params`, `cutoff`, `skin`,
+`pairlist_threshold`, `rcut`, `alpha`, `k`, `exclude`, `rebuilds`, `_vl.rebuilds`) and the Lorentz-Berthelot
+`_tables` are inherited, so accusim code that reads them or checks `isinstance` against the reference classes
+sees the same objects. `compute(system) -> (F[n, 3] float64 N, U float J)` keeps the reference contract; the
+pair search and the pair loops run as FP64 CUDA kernels in libaccusim_b200.so. On a `GpuSystem` the device
+copy of the positions is used directly.
 """
 from __future__ import annotations
 
@@ -15,20 +17,9 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._accusim import forces as _af
 from .device import DevStatus, Workspace, require_cuda, stream_handle, to_dev
-from .system import species_arrays
-from .units import k_e, si
-
-
-class Force:
-    """Plug-in base with the reference's class flags (accusim/forces.py:15-21)."""
-
-    conservative = True
-    external = False
-    central = True
-
-    def compute(self, system):
-        raise NotImplementedError
+from .state import is_gpu_system
 
 
 def _check_system(s):
@@ -53,11 +44,11 @@ class DeviceNeighborList:
         self.ws = Workspace()
         self.status = None
 
-    def _capacity(self, s, pos_d, R):
+    def _capacity(self, s, R, lo=None, hi=None):
         if s.box is not None:
             vol = float(np.prod(s.box))
         else:
-            ext = np.maximum(np.ptp(s.pos, axis=0), R)
+            ext = np.maximum(hi - lo, R)
             vol = float(np.prod(ext))
         expected = s.n / max(vol, 1e-300) * 4.0 / 3.0 * math.pi * R ** 3
         return int(min(max(expected * 1.35 + 24, 16), s.n - 1 if s.n > 1 else 1) + 7) // 8 * 8
@@ -68,9 +59,10 @@ class DeviceNeighborList:
         n = s.n
         g = _lib.AcsGrid()
         boxarr, boxp, periodic = _box_args(s)
-        if s.box is None:
-            lo = np.ascontiguousarray(s.pos.min(axis=0), dtype=np.float64)
-            hi = np.ascontiguousarray(s.pos.max(axis=0), dtype=np.float64)
+        lo = hi = None
+        if s.box is None:   # open box: the grid spans the particles' extent
+            ext = torch.stack([pos_d.min(dim=0).values, pos_d.max(dim=0).values]).cpu().numpy()
+            lo, hi = np.ascontiguousarray(ext[0]), np.ascontiguousarray(ext[1])
             lop, hip = lo.ctypes.data, hi.ctypes.data
         else:
             lop = hip = None
@@ -79,7 +71,7 @@ class DeviceNeighborList:
         wbytes = L.acs_nlist_work_bytes(n, C.byref(g))
         if self.status is None:
             self.status = DevStatus()
-        maxnb = max(self.maxnb, self._capacity(s, pos_d, R))
+        maxnb = max(self.maxnb, self._capacity(s, R, lo, hi))
         for _ in range(4):
             npad = (n + 31) // 32 * 32
             if self.nbr is None or self.nbr.numel() < npad * maxnb:
@@ -124,10 +116,17 @@ class VerletList:
         self.rebuilds = 0
         self._flag = None
 
+    def _same_ids(self, s, st):
+        """ids unchanged since the last build (a GpuSystem whose ids were not touched needs no comparison)."""
+        if is_gpu_system(s) and st["ids_version"] == (id(s), s.ids_version()):
+            return True
+        ids = s.ids
+        return st["ids"].shape == ids.shape and np.array_equal(st["ids"], ids)
+
     def pairs(self, s, pos_d, rc, skin) -> DeviceNeighborList:
         st = self._state
-        if st is not None and st["ids"].shape == s.ids.shape and np.array_equal(st["ids"], s.ids) \
-                and np.array_equal(st["box"], s.box) and st["rc"] == rc and skin > 0:
+        if st is not None and self._same_ids(s, st) and np.array_equal(st["box"], s.box) and st["rc"] == rc \
+                and skin > 0:
             if self._flag is None:
                 self._flag = torch.zeros(1, dtype=torch.int32, device="cuda")
             boxarr, boxp, periodic = _box_args(s)
@@ -138,8 +137,9 @@ class VerletList:
                 return st["list"]
         nl = st["list"] if st is not None else DeviceNeighborList()
         nl.build(s, pos_d, rc + skin)
-        self._state = dict(list=nl, pos0=pos_d.clone(), ids=s.ids.copy(),
-                           box=None if s.box is None else s.box.copy(), rc=rc)
+        ids = s.ids.copy()
+        self._state = dict(list=nl, pos0=pos_d.clone(), ids=ids, box=None if s.box is None else s.box.copy(), rc=rc,
+                           ids_version=(id(s), s.ids_version()) if is_gpu_system(s) else None)
         self.rebuilds += 1
         return nl
 
@@ -155,37 +155,15 @@ class _Scratch:
         return self.energy
 
 
-class LennardJones(Force):
-    """12-6 Lennard-Jones with Lorentz-Berthelot mixing, truncated at cutoff*sigma_ij with the energy
-    shifted to zero there (accusim/forces.py:101-175). params: {species: (epsilon J, sigma m)}; species
-    not listed do not interact. `cutoff`, `skin` in units of sigma; N >= pairlist_threshold uses the
-    Verlet list, smaller systems the dense all-pairs kernel."""
+class LennardJones(_af.LennardJones):
+    """accusim's 12-6 Lennard-Jones (Lorentz-Berthelot mixing, energy shifted to zero at cutoff*sigma_ij) with
+    its pair search and pair loop on the GPU: the Verlet list for n >= pairlist_threshold, the dense all-pairs
+    kernel below."""
 
     def __init__(self, params: dict, cutoff: float = 2.5, pairlist_threshold: int = 400, skin: float = 0.3):
-        self.params = {k: (si(e, "J"), si(sg, "m")) for k, (e, sg) in params.items()}
-        self.cutoff = cutoff
-        self.pairlist_threshold = pairlist_threshold
-        self.skin = skin
+        super().__init__(params, cutoff=cutoff, pairlist_threshold=pairlist_threshold, skin=skin)
         self._vl = VerletList()
         self._scr = _Scratch()
-
-    @property
-    def rebuilds(self):
-        return self._vl.rebuilds
-
-    def _tables(self, s):
-        """Lorentz-Berthelot tables (accusim/forces.py:144-155)."""
-        k = len(s.species)
-        eps = np.zeros((k, k))
-        sig = np.ones((k, k))
-        for a, A in enumerate(s.species):
-            for b, B in enumerate(s.species):
-                if A.name in self.params and B.name in self.params:
-                    ea, sa = self.params[A.name]
-                    eb, sb = self.params[B.name]
-                    eps[a, b] = np.sqrt(ea * eb)
-                    sig[a, b] = 0.5 * (sa + sb)
-        return eps, sig
 
     def list_radius(self, s):
         eps_t, sig_t = self._tables(s)
@@ -220,35 +198,38 @@ class LennardJones(Force):
 
     def compute(self, s):
         if s.n < 2:
-            return np.zeros_like(s.pos), 0.0
+            return np.zeros((s.n, s.dim)), 0.0
         _check_system(s)
         require_cuda()
-        F, E = self.compute_device(s, to_dev(s.pos), to_dev(s.sp, torch.int32))
+        F, E = self.compute_device(s, *_device_positions(s))
         return F.cpu().numpy(), float(E.item())
 
 
-class DampedShiftedCoulomb(Force):
-    """Damped shifted force electrostatics (Fennell & Gezelter 2006): pair potential erfc(a r)/r shifted
-    so energy and force vanish at rcut, plus the self term (accusim/forces.py:391-452). `exclude` lists id
-    pairs with no interaction; `skin` defaults to 0.15 rcut."""
+class DampedShiftedCoulomb(_af.DampedShiftedCoulomb):
+    """accusim's damped shifted force electrostatics (Fennell & Gezelter 2006; `exclude` id pairs, skin 0.15
+    rcut by default) with its pair search and pair loop on the GPU."""
 
-    def __init__(self, rcut, alpha=None, k=k_e, pairlist_threshold=400, exclude=(), skin=None):
-        self.pairlist_threshold = pairlist_threshold
-        self.exclude = [tuple(p) for p in exclude]
-        self.k = si(k, "J*m/C^2")
-        self.rcut = si(rcut, "m")
-        self.alpha = 2.0 / self.rcut if alpha is None else si(alpha, "1/m")
-        self.skin = 0.15 * self.rcut if skin is None else si(skin, "m")
+    def __init__(self, rcut, alpha=None, k=None, pairlist_threshold=400, exclude=(), skin=None):
+        kw = {} if k is None else {"k": k}
+        super().__init__(rcut, alpha=alpha, pairlist_threshold=pairlist_threshold, exclude=exclude, skin=skin, **kw)
         self._vl = VerletList()
         self._scr = _Scratch()
 
-    @property
-    def rebuilds(self):
-        return self._vl.rebuilds
-
     def _exclusion_csr(self, s):
+        """Excluded pairs as a CSR table by atom index, both directions (device int32), or (None, None). Cached
+        for a GpuSystem whose ids were not touched since."""
         if not self.exclude:
             return None, None
+        key = (id(s), s.ids_version(), len(self.exclude)) if is_gpu_system(s) else None
+        cached = getattr(self, "_ex_cache", None)
+        if key is not None and cached is not None and cached[0] == key:
+            return cached[1]
+        out = self._exclusion_table(s)
+        if key is not None:
+            self._ex_cache = (key, out)
+        return out
+
+    def _exclusion_table(self, s):
         where = {int(pid): k for k, pid in enumerate(s.ids)}
         ex = [(where[a], where[b]) for a, b in self.exclude if a in where and b in where]
         if not ex:
@@ -263,17 +244,20 @@ class DampedShiftedCoulomb(Force):
         start = np.cumsum(start).astype(np.int32)
         return to_dev(start), to_dev(dst.astype(np.int32))
 
-    def compute_device(self, s, pos_d, q_d=None):
+    def compute_device(self, s, pos_d):
+        """Forces as a device tensor (n, 3) and the energy as a device scalar."""
         n = s.n
         F = torch.empty((n, 3), dtype=torch.float64, device="cuda")
         E = self._scr.energy_buf()
-        q = s.charges
-        if not np.any(q):
+        if is_gpu_system(s):
+            q_d, charged = s.device_charges()
+        else:
+            q = np.asarray(s.charges, dtype=np.float64)
+            q_d, charged = to_dev(q), bool(np.any(q))
+        if not charged:
             F.zero_()
             E.zero_()
             return F, E
-        if q_d is None or q_d.dtype != torch.float64:
-            q_d = to_dev(q.astype(np.float64))
         nl = None
         if n >= self.pairlist_threshold:
             nl = self._vl.pairs(s, pos_d, self.rcut, self.skin)
@@ -292,18 +276,25 @@ class DampedShiftedCoulomb(Force):
     def compute(self, s):
         q = s.charges
         if not np.any(q):
-            return np.zeros_like(s.pos), 0.0
+            return np.zeros((s.n, s.dim)), 0.0
         _check_system(s)
         require_cuda()
-        F, E = self.compute_device(s, to_dev(s.pos))
+        F, E = self.compute_device(s, _device_positions(s)[0])
         return F.cpu().numpy(), float(E.item())
+
+
+def _device_positions(s):
+    """(positions, species) of a system as device tensors: a GpuSystem's resident copy, else one upload."""
+    if is_gpu_system(s):
+        return s.device_state()[0], s.device_species()
+    return to_dev(np.asarray(s.pos, dtype=np.float64)), to_dev(np.asarray(s.sp), torch.int32)
 
 
 def cell_list_pairs(s, rc):
     """All pairs (i < j) closer than rc, found on the device (accusim/forces.py:279-321)."""
     _check_system(s)
     require_cuda()
-    nl = DeviceNeighborList().build(s, to_dev(s.pos), rc)
+    nl = DeviceNeighborList().build(s, _device_positions(s)[0], rc)
     i, j = nl.pairs(s.n)
     order = np.lexsort((j, i))
     return i[order], j[order]

@@ -1,9 +1,15 @@
-"""GPU drop-ins for accusim's `VelocityVerlet`, `Langevin` and `NoseHoover` (accusim/integrators.py:9-116).
+"""GPU drop-ins for accusim's `VelocityVerlet`, `Langevin` and `NoseHoover` (accusim/integrators.py:19-116).
 
-`step(sim, dt)` performs kick-drift-wrap-force-kick with FP64 kernels in the reference's IEEE operation
-order (no FMA), so given the same accelerations it is bit-identical to the reference step. When every
-force of the simulation is a GPU plug-in the forces are evaluated on the device positions directly;
-otherwise `sim.update_forces()` runs the plug-in protocol unchanged.
+The classes subclass accusim's own (class flags, constructor arguments, the Nose-Hoover thermostat state and its
+half-steps `_half`, `dof`, `bath_energy` are inherited) and replace the kick-drift-wrap-force-kick with FP64
+kernels in the reference's IEEE operation order (no FMA): given the same accelerations a step is bit-identical
+to the reference's. When every force of the simulation is one of this package's GPU plug-ins the forces are
+evaluated on the device positions directly; otherwise `sim.update_forces()` runs accusim's plug-in protocol.
+
+On a `GpuSystem` the state stays on the device across steps: positions, velocities and accelerations are not
+copied back; `sim.force` and `sim.acc` are refreshed when the host next reads the system (accusim's
+`Simulation.record` does), and only the potential energy `sim.pe` (a float in accusim's contract) is read back
+every step. On any other accusim `System` each step uploads the state and downloads it again.
 """
 from __future__ import annotations
 
@@ -11,18 +17,10 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._accusim import integrators as _ai
 from .device import require_cuda, stream_handle, to_dev
-from .units import k_B, si
-
-
-class Integrator:
-    order = 1
-    symplectic = False
-    stochastic = False
-    thermostat = False
-
-    def step(self, sim, dt):
-        raise NotImplementedError
+from .state import is_gpu_system
+from .units import k_B
 
 
 def _masses_table(s):
@@ -30,7 +28,8 @@ def _masses_table(s):
 
 
 def device_forces(sim, pos_d, sp_d):
-    """Sum of the forces of `sim` on device positions; None if some force is not a GPU plug-in."""
+    """Sum of the forces of `sim` on device positions as (F (n, 3), U (1,)) device tensors; None if some force
+    is not one of this package's GPU plug-ins."""
     from .forces import DampedShiftedCoulomb, LennardJones
     s = sim.system
     F = None
@@ -50,141 +49,123 @@ def device_forces(sim, pos_d, sp_d):
     return F, U
 
 
-def _begin(sim):
-    """Upload the state for a device step: (library, stream, n, pos, vel, acc) device tensors."""
-    s = sim.system
-    if s.dim != 3:
-        raise ValueError("accusim_b200 integrators handle 3-dimensional systems")
-    require_cuda()
-    return (_lib.lib(), stream_handle(), s.n, to_dev(s.pos), to_dev(s.vel),
-            to_dev(np.asarray(sim.acc, dtype=np.float64)))
+class _DeviceStep:
+    """One integrator step's device state: positions, velocities, accelerations and species of `sim.system`
+    on the GPU (the resident copy of a GpuSystem, else uploaded from the host arrays)."""
 
+    def __init__(self, sim):
+        s = sim.system
+        if s.dim != 3:
+            raise ValueError("accusim_b200 integrators handle 3-dimensional systems")
+        require_cuda()
+        self.sim, self.s = sim, s
+        self.L, self.st, self.n = _lib.lib(), stream_handle(), s.n
+        self.resident = is_gpu_system(s)
+        if self.resident:
+            self.pos, self.vel = s.device_state()
+            acc = s.device_acc()
+            self.acc = acc if acc is not None else to_dev(np.asarray(sim.acc, dtype=np.float64))
+            self.sp = s.device_species()
+        else:
+            self.pos, self.vel = to_dev(s.pos), to_dev(s.vel)
+            self.acc = to_dev(np.asarray(sim.acc, dtype=np.float64))
+            self.sp = None
 
-def _drift(L, st, s, pos_d, vel_d, n, dt, wrap):
-    """pos += dt * vel, then pos %= box for periodic boxes when `wrap`."""
-    boxarr, boxp = _lib.dbl3(s.box) if (wrap and s.box is not None) else (None, None)
-    periodic = 1 if (wrap and s.box is not None and s.periodic) else 0
-    _lib.check(L.acs_vv_drift_wrap(pos_d.data_ptr(), vel_d.data_ptr(), n, float(dt), boxp, periodic, st),
-               "acs_vv_drift_wrap")
+    def kick(self, h):
+        """vel += h * acc"""
+        _lib.check(self.L.acs_vv_kick(self.vel.data_ptr(), self.acc.data_ptr(), self.n, h, self.st), "acs_vv_kick")
 
+    def drift(self, dt, wrap):
+        """pos += dt * vel, then pos %= box for periodic boxes when `wrap`."""
+        s = self.s
+        boxarr, boxp = _lib.dbl3(s.box) if (wrap and s.box is not None) else (None, None)
+        periodic = 1 if (wrap and s.box is not None and s.periodic) else 0
+        _lib.check(self.L.acs_vv_drift_wrap(self.pos.data_ptr(), self.vel.data_ptr(), self.n, float(dt), boxp,
+                                            periodic, self.st), "acs_vv_drift_wrap")
 
-def _finish(sim, L, st, pos_d, vel_d, acc_d, h):
-    """Walls, forces at the new positions (device plug-ins, else the plug-in protocol), the closing kick
-    and the download: accusim/integrators.py:29-31."""
-    s = sim.system
-    n = s.n
-    if s.box is not None and not s.periodic:
-        # elastic walls: the reference's reflection and wall-impulse ledger (accusim/system.py:130-140)
-        s.pos = pos_d.cpu().numpy()
-        s.vel = vel_d.cpu().numpy()
-        s.apply_boundaries()
-        pos_d, vel_d = to_dev(s.pos), to_dev(s.vel)
-    sp_d = to_dev(s.sp, torch.int32)
-    res = device_forces(sim, pos_d, sp_d)
-    if res is None:
-        s.pos = pos_d.cpu().numpy()
-        s.vel = vel_d.cpu().numpy()
-        sim.update_forces()
-        acc_d = to_dev(np.asarray(sim.acc, dtype=np.float64))
-    else:
-        F_d, U_d = res
+    def forces_and_kick(self, h):
+        """Walls, forces at the new positions (device plug-ins, else the plug-in protocol on host arrays), the
+        closing kick, and the hand-back of the state: accusim/integrators.py:29-31."""
+        sim, s = self.sim, self.s
+        walls = s.box is not None and not s.periodic
+        sp = self.sp if self.sp is not None else to_dev(np.asarray(s.sp), torch.int32)
+        res = None if walls else device_forces(sim, self.pos, sp)
+        if res is None:
+            # elastic walls (accusim/system.py:130-140) or a force without a device path: host protocol
+            s.pos = self.pos.cpu().numpy()
+            s.vel = self.vel.cpu().numpy()
+            if walls:
+                s.apply_boundaries()
+            sim.update_forces()
+            self.vel = to_dev(s.vel)
+            self.acc = to_dev(np.asarray(sim.acc, dtype=np.float64))
+            self.kick(h)
+            s.vel = self.vel.cpu().numpy()
+            return
+        F, U = res
         m = _masses_table(s)
-        _lib.check(L.acs_vv_accel(acc_d.data_ptr(), F_d.data_ptr(), sp_d.data_ptr(), m.ctypes.data, len(m), n,
-                                  st), "acs_vv_accel")
-        s.pos = pos_d.cpu().numpy()
-        sim.force = F_d.cpu().numpy()
-        sim.pe = float(U_d.item())
-        sim.acc = acc_d.cpu().numpy()
-    _lib.check(L.acs_vv_kick(vel_d.data_ptr(), acc_d.data_ptr(), n, h, st), "acs_vv_kick")
-    s.vel = vel_d.cpu().numpy()
+        _lib.check(self.L.acs_vv_accel(self.acc.data_ptr(), F.data_ptr(), sp.data_ptr(), m.ctypes.data, len(m),
+                                       self.n, self.st), "acs_vv_accel")
+        self.kick(h)
+        sim.pe = float(U.item())
+        if self.resident:
+            mirrors = []
+            for name, dev in (("force", F), ("acc", self.acc)):
+                host = getattr(sim, name, None)
+                if not (isinstance(host, np.ndarray) and host.shape == (self.n, 3) and host.dtype == np.float64):
+                    host = np.empty((self.n, 3))
+                    setattr(sim, name, host)
+                mirrors.append((host, dev))
+            s.stepped_on_device(self.acc, F, mirrors)
+        else:
+            s.pos = self.pos.cpu().numpy()
+            sim.force = F.cpu().numpy()
+            sim.acc = self.acc.cpu().numpy()
+            s.vel = self.vel.cpu().numpy()
 
 
-class VelocityVerlet(Integrator):
-    """Kick-drift-kick leapfrog: 2nd order, symplectic, time reversible."""
-
-    order = 2
-    symplectic = True
+class VelocityVerlet(_ai.VelocityVerlet):
+    """accusim's kick-drift-kick leapfrog (2nd order, symplectic) with the step on the GPU."""
 
     def step(self, sim, dt):
-        L, st, n, pos_d, vel_d, acc_d = _begin(sim)
+        d = _DeviceStep(sim)
         h = 0.5 * dt
-        _lib.check(L.acs_vv_kick(vel_d.data_ptr(), acc_d.data_ptr(), n, h, st), "acs_vv_kick")
-        _drift(L, st, sim.system, pos_d, vel_d, n, dt, True)
-        _finish(sim, L, st, pos_d, vel_d, acc_d, h)
+        d.kick(h)
+        d.drift(dt, True)
+        d.forces_and_kick(h)
 
 
-class Langevin(Integrator):
-    """BAOAB Langevin dynamics (Leimkuhler-Matthews), accusim/integrators.py:50-71: samples temperature T.
+class Langevin(_ai.Langevin):
+    """accusim's BAOAB Langevin dynamics (Leimkuhler-Matthews) with B and A on the GPU.
 
-    Same operations in the same IEEE order as the reference, with the normal draws taken from `sim.rng` as
-    the reference takes them, so a step is bit-identical to the reference's given the same accelerations and
-    generator state. B and A run on the device (acs_vv_kick, acs_vv_drift_wrap), O is acs_langevin_ou."""
-
-    order = 2
-    stochastic = True
-    thermostat = True
-
-    def __init__(self, temperature, friction):
-        self.T = si(temperature, "K")
-        self.gamma = si(friction, "1/s")
+    The normal draws come from `sim.rng` exactly as the reference takes them, and the O-step runs as
+    acs_langevin_ou in the reference's operation order, so a step is bit-identical to the reference's given the
+    same accelerations and generator state."""
 
     def step(self, sim, dt):
         s = sim.system
-        L, st, n, pos_d, vel_d, acc_d = _begin(sim)
+        d = _DeviceStep(sim)
         h = 0.5 * dt
-        _lib.check(L.acs_vv_kick(vel_d.data_ptr(), acc_d.data_ptr(), n, h, st), "acs_vv_kick")
-        _drift(L, st, s, pos_d, vel_d, n, h, False)
+        d.kick(h)
+        d.drift(h, False)
         c1 = np.exp(-self.gamma * dt)
-        sig = np.ascontiguousarray(np.sqrt((1 - c1 ** 2) * k_B * self.T / s.masses), dtype=np.float64)
-        noise = to_dev(np.ascontiguousarray(sim.rng.normal(size=s.vel.shape), dtype=np.float64))
+        masses = _masses_table(s)[np.asarray(s.host_species() if d.resident else s.sp)]
+        sig = np.ascontiguousarray(np.sqrt((1 - c1 ** 2) * k_B * self.T / masses), dtype=np.float64)
+        noise = to_dev(np.ascontiguousarray(sim.rng.normal(size=(d.n, s.dim)), dtype=np.float64))
         sig_d = to_dev(sig)
-        _lib.check(L.acs_langevin_ou(vel_d.data_ptr(), noise.data_ptr(), sig_d.data_ptr(), n, float(c1), st),
+        _lib.check(d.L.acs_langevin_ou(d.vel.data_ptr(), noise.data_ptr(), sig_d.data_ptr(), d.n, float(c1), d.st),
                    "acs_langevin_ou")
-        _drift(L, st, s, pos_d, vel_d, n, h, True)
-        _finish(sim, L, st, pos_d, vel_d, acc_d, h)
+        d.drift(h, True)
+        d.forces_and_kick(h)
 
 
-class NoseHoover(Integrator):
-    """Nose-Hoover thermostat with the Trotter splitting of accusim/integrators.py:74-116 (Martyna-Tuckerman-
-    Klein): canonical sampling with the conserved extended energy E + Q xi^2 / 2 + N_f kT eta.
-
-    The thermostat half-steps are O(n) scalar updates on the host arrays, with the reference's NumPy
-    expressions (so the kinetic-energy sum has the reference's summation order); the VelocityVerlet step
-    between them runs on the device. `period` sets the thermostat mass Q = N_f kT period^2."""
-
-    order = 2
-    thermostat = True
-
-    def __init__(self, temperature, period):
-        self.T = si(temperature, "K")
-        self.tau = si(period, "s")
-        self.xi = 0.0
-        self.eta = 0.0
-        self.Q = None
-        self._vv = VelocityVerlet()
-
-    @staticmethod
-    def dof(s):
-        return s.dim * max(s.n - 1, 1)
-
-    def _half(self, s, dt):
-        kT, nf = k_B * self.T, self.dof(s)
-        if self.Q is None:
-            self.Q = nf * kT * self.tau ** 2
-        k2 = float(np.sum(s.masses[:, None] * s.vel ** 2))
-        self.xi += 0.25 * dt * (k2 - nf * kT) / self.Q
-        scale = np.exp(-0.5 * dt * self.xi)
-        s.vel *= scale
-        self.eta += 0.5 * dt * self.xi
-        self.xi += 0.25 * dt * (k2 * scale ** 2 - nf * kT) / self.Q
+class NoseHoover(_ai.NoseHoover):
+    """accusim's Nose-Hoover thermostat (Trotter splitting, Martyna-Tuckerman-Klein): the thermostat half-steps
+    are accusim's own (`_half`, on the host arrays, so the kinetic-energy sum keeps the reference's summation
+    order); the VelocityVerlet step between them runs on the GPU."""
 
     def step(self, sim, dt):
         s = sim.system
         self._half(s, dt)
-        self._vv.step(sim, dt)
+        VelocityVerlet.step(self, sim, dt)
         self._half(s, dt)
-
-    def bath_energy(self, s):
-        if self.Q is None:
-            return 0.0
-        return 0.5 * self.Q * self.xi ** 2 + self.dof(s) * k_B * self.T * self.eta

@@ -295,8 +295,8 @@ class LearnedCorrection:
         self.enabled = True
 
     def _system(self, data, k):
-        from .system import System
-        s = System(3, box=data["box"], periodic=True)
+        from ._accusim import system as _asys
+        s = _asys.System(3, box=data["box"], periodic=True)
         for name, m, q in data["species"]:
             s.add_species(name, m, charge=q)
         s.pos = data["pos"][k]

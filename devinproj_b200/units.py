@@ -1,27 +1,13 @@
-"""SI conversion at the API edge and the CODATA constants the path uses.
-
-Arguments may be plain SI numbers or any quantity object exposing `.si(unit)` (accusim's
-`Quantity`, accusim/units.py:123-129); `si()` mirrors accusim/units.py:219-223.
-"""
+"""SI values of accusim's physical constants (accusim/units.py:226-233) as plain floats for the host code and the
+engine's unit conversion, and accusim's own `si()` for arguments given as quantities."""
 from __future__ import annotations
 
-import math
+from ._accusim import units as _u
 
-import numpy as np
-
-k_B = 1.380649e-23              # J/K
-N_A = 6.02214076e23             # 1/mol
-e_charge = 1.602176634e-19      # C
-epsilon_0 = 8.8541878128e-12    # C^2/J/m
-k_e = 1 / (4 * math.pi * epsilon_0)
-amu = 1.66053906660e-27         # kg
-c_light = 299792458.0           # m/s
-
-
-def si(x, unit=None):
-    """SI number from a quantity (checked by its own `.si`) or a plain number passed through."""
-    if hasattr(x, "si") and callable(getattr(x, "si")):
-        return x.si(unit)
-    if hasattr(x, "value") and hasattr(x, "dim"):
-        return x.value
-    return np.asarray(x, dtype=float) if not np.isscalar(x) else float(x)
+si = _u.si
+k_B = float(_u.k_B.value)                         # J/K
+N_A = float(_u.N_A.value)                         # 1/mol
+e_charge = float(_u.e_charge.value)               # C
+k_e = float(_u.k_e.value)                         # J m / C^2
+amu = float(_u.parse_unit("u").value)             # kg
+c_light = float(_u.c.value)                       # m/s

@@ -7,6 +7,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+# accusim, the framework the plug-ins plug into, from the repository's offline install (baseline/_ref) when it is
+# not installed in the environment
+import devinproj_b200._accusim  # noqa: E402,F401
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 

@@ -114,7 +114,9 @@ def test_engine_config_validation_is_host_side():
 def test_engine_dsf_exclusion_tables():
     """DSF exclusions: the engine's CSR table by atom index (ids mapped through system.ids, both directions,
     pairs with an unknown id dropped) and its host-side validation in acs_engine_bytes."""
-    from devinproj_b200 import DampedShiftedCoulomb, System
+    from accusim import System
+
+    from devinproj_b200 import DampedShiftedCoulomb
     from devinproj_b200 import engine as E
     from devinproj_b200.engine import ENGINE_SIGNATURES, dsf_exclusions
     s = System(3, box=20.0, periodic=True)
@@ -177,6 +179,12 @@ def test_engine_erfc_approximation_bound():
     tf = f(1) / (f(1) + f(p) * xf)
     qf = tf * (f(a1) + tf * (f(a2) + tf * (f(a3) + tf * (f(a4) + tf * f(a5)))))
     assert np.max(np.abs((qf * np.exp(-(xf * xf))).astype(np.float64) - erfc(x))) <= 7e-7
+    # the host copy behind the DSF shift constants (erfc(alpha rc)) carries the same coefficients, so the
+    # engine's shifted DSF term vanishes at rc under the approximation it evaluates
+    host = src[src.index("double erfc_as_host(double x)"):]
+    host = host[:host.index("\n}")]
+    ch = [float(v) for v in re.findall(r"(-?\d+\.\d+)", host) if float(v) != 1.0]
+    assert ch == [p, a5, a4, a3, a2, a1]
 
 
 def test_default_threads_per_atom_follow_measured_optima():

@@ -16,7 +16,7 @@ TOL = 1e-12
 
 
 def product_system(g, suffix=""):
-    from devinproj_b200 import System
+    from accusim import System
     box = g["box" + suffix] if bool(g["has_box" + suffix]) else None
     s = System(3, box=box, periodic=bool(g["periodic" + suffix]))
     for name, m, q in zip(g["species" + suffix], g["masses" + suffix], g["charges" + suffix]):
@@ -91,7 +91,8 @@ def test_lj_fp64_matches_reference(golden, kind):
 def test_lj_verlet_skin_matches_reference_along_trajectory(golden):
     """Skin list == fresh list along a VV run, and the rebuild count equals the reference's
     (tests/test_nose_hoover.py:51-60)."""
-    from devinproj_b200 import LennardJones, Simulation, VelocityVerlet
+    from accusim import Simulation
+    from devinproj_b200 import LennardJones, VelocityVerlet
     g = golden("lj500_skin")
     s = product_system(g, "0")
     eps, sig = float(g["eps"]), float(g["sig"])
@@ -113,7 +114,8 @@ def test_lj_verlet_skin_matches_reference_along_trajectory(golden):
 
 def test_velocity_verlet_matches_reference_trajectory(golden):
     """60 VV steps of the 864-atom argon case through Simulation.run with the drop-ins."""
-    from devinproj_b200 import LennardJones, Simulation, VelocityVerlet
+    from accusim import Simulation
+    from devinproj_b200 import LennardJones, VelocityVerlet
     g = golden("argon864")
     s = product_system(g, "0")
     lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
@@ -192,7 +194,8 @@ def test_dsf_exclusions_match_reference(golden):
 
 def test_dsf_verlet_skin_matches_reference_rebuilds(golden):
     """tests/test_dsf.py:119-139: 30 perturbations regenerated from the same seed."""
-    from devinproj_b200 import DampedShiftedCoulomb, System
+    from accusim import System
+    from devinproj_b200 import DampedShiftedCoulomb
     g = golden("dsf_skin")
     n = 8
     s = System(3, box=float(n), periodic=True)
@@ -218,7 +221,8 @@ def test_dsf_verlet_skin_matches_reference_rebuilds(golden):
 
 
 def test_nacl4096_lj_plus_dsf_matches_reference(golden):
-    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, Simulation, VelocityVerlet
+    from accusim import Simulation
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, VelocityVerlet
     g = golden("nacl4096")
     params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
     s = product_system(g)
@@ -239,7 +243,8 @@ def test_nacl4096_lj_plus_dsf_matches_reference(golden):
 
 def test_forces_are_negative_gradient_and_newton3():
     """tests/test_forces.py:30-52 on the GPU plug-ins: central differences of U and sum F = 0."""
-    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, System
+    from accusim import System
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones
     rng = np.random.default_rng(0)
     for periodic in (False, True):
         s = System(3, box=2e-9 if periodic else None, periodic=periodic)
@@ -265,7 +270,8 @@ def test_forces_are_negative_gradient_and_newton3():
 
 
 def test_lj_minimum_and_small_systems():
-    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, System
+    from accusim import System
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones
     s = System(3)
     s.add_species("Ar", 6.6e-26)
     sigma = 3.4e-10
@@ -285,7 +291,7 @@ def test_lj_minimum_and_small_systems():
 
 def _rocksalt(n):
     """Unit-charge rock salt on the integer grid, unit masses and box n (tests/test_dsf.py:7-15)."""
-    from devinproj_b200 import System
+    from accusim import System
     s = System(3, box=float(n), periodic=True)
     s.add_species("Na", 1.0, charge=1.0)
     s.add_species("Cl", 1.0, charge=-1.0)
@@ -301,7 +307,8 @@ def test_dsf_known_answers():
     energy of rock salt within 2e-3 at rc 3.9, alpha 0.6; forces are the energy's gradient and sum to
     zero; a pair just inside the cutoff feels no force and its energy is the self term; on a disordered
     melt the energy is within 3% of Ewald's (the device Ewald, itself pinned to the reference)."""
-    from devinproj_b200 import DampedShiftedCoulomb, System
+    from accusim import System
+    from devinproj_b200 import DampedShiftedCoulomb
     from devinproj_b200.ewald import Ewald
     s = _rocksalt(8)
     _, U = DampedShiftedCoulomb(rcut=3.9, alpha=0.6, k=1.0).compute(s)
@@ -340,7 +347,7 @@ def test_dsf_known_answers():
 
 def test_list_capacity_overflow_regrows():
     """A dense clump far above the capacity estimate: the build reports overflow and is redone bigger."""
-    from devinproj_b200 import System
+    from accusim import System
     from devinproj_b200.forces import DeviceNeighborList
     from devinproj_b200.device import to_dev
     rng = np.random.default_rng(2)
@@ -362,7 +369,8 @@ def test_dropin_thermostats_match_reference(golden, kind):
     plug-ins inside `Simulation.run`: 40 steps of 108 argon atoms against the reference's run. The device
     FP64 forces differ from the reference's at round-off (summation order), so the trajectories agree to
     the VelocityVerlet trajectory test's 1e-9, not bitwise; the report gains its thermostat rows."""
-    from devinproj_b200 import Langevin, LennardJones, NoseHoover, Simulation
+    from accusim import Simulation
+    from devinproj_b200 import Langevin, LennardJones, NoseHoover
     g = golden("thermostats108")
     s = product_system(g, "0")
     lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
@@ -389,7 +397,8 @@ def test_accuracy_report_matches_reference(golden, case):
     and a 512-ion NaCl melt (LJ + DSF, 20 steps: two species' timescales and the DSF vs Ewald row). The same
     rows and grades; values to 1e-6 relative where they are not round-off (the device FP64 forces differ from
     NumPy's at round-off and the runs are short)."""
-    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, Simulation, VelocityVerlet
+    from accusim import Simulation
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, VelocityVerlet
     g = golden(case)
     s = product_system(g)
     if case == "report_argon108":
@@ -412,7 +421,7 @@ def test_accuracy_report_matches_reference(golden, case):
         else:
             assert abs(c.value - v) <= 1e-6 * abs(v), (c.name, c.value, v)
     # accusim/advisor.py:51-55 on the same end-of-run state: the shortest timescale / 100
-    from devinproj_b200 import suggest_dt
+    from accusim import suggest_dt
     ratio = float(g["values"][list(g["names"]).index("timestep vs physics")])
     assert suggest_dt(sim) == pytest.approx(float(g["dt"]) / ratio / 100, rel=1e-6)
 

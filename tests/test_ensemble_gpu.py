@@ -49,7 +49,8 @@ def test_richardson_order_matches_fp64_oracle():
 
 
 def test_calibrate_dt_ensemble_matches_sequential_fp64():
-    from devinproj_b200 import Simulation, VelocityVerlet, calibrate_dt, configs
+    from accusim import Simulation, calibrate_dt
+    from devinproj_b200 import VelocityVerlet, configs
     from devinproj_b200.ensemble import calibrate_dt_ensemble
     s, lj = configs.lj_fluid(5, seed=1)
     dt0 = 0.04 * configs.AR_TAU
@@ -116,7 +117,8 @@ def test_calibrate_dt_matches_reference(golden):
     1e-5): from dt = 40 fs the plug-in halves to the reference's dt, with its drift; with dt unset it starts
     from suggest_dt, as the reference does; the batched engine form reaches the same dt (in this 17 A box the
     list radius exceeds half the box, so the engine rebuilds its lists every step)."""
-    from devinproj_b200 import LennardJones, Simulation, VelocityVerlet, calibrate_dt
+    from accusim import Simulation, calibrate_dt
+    from devinproj_b200 import LennardJones, VelocityVerlet
     from devinproj_b200.ensemble import calibrate_dt_ensemble
     from tests.test_dropin_gpu import product_system
     g = golden("calibrate_argon108")

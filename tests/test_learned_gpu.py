@@ -32,7 +32,7 @@ def test_ewald_matches_reference_on_disordered_melt(golden):
 @pytest.mark.parametrize("cells", [1, 2])
 def test_ewald_madelung_known_answer(cells):
     """tests/test_forces.py:90-97: NaCl Madelung constant 1.747564594633, forces vanish on the lattice."""
-    from devinproj_b200 import System
+    from accusim import System
     from devinproj_b200.ewald import Ewald
     s = System(3, box=2.0 * cells, periodic=True)
     s.add_species("Na", 1.0, charge=1.0)
