@@ -7,8 +7,11 @@ dt* 0.005), FP32-compensated pair forces with FP64 integration, the step loop as
 one VelocityVerlet step of the whole system (forces, both kicks, drift, skin test, list rebuilds when due).
 Inputs (positions, velocities, 400+ MB of neighbour lists) exceed the 126 MB L2, so no flush is needed.
 Under torchrun each rank advances its own independent system (replicas only; no collective in the step
-loop) and rank 0 prints one JSON line. `--impl reference` times the CPU restatement of the reference
-NumPy path on this host's cores (all of them, one process each) for the same metric.
+loop), or, for the replica ensemble, its shard of the replicas; rank 0 prints one JSON line. The line also
+carries the energy drift of a fixed 10^4-step window and the throughput of the plain FP64 plug-ins running
+device-resident inside accusim's own Simulation.run (the denominator of the FP32c path's speed-up).
+`--impl reference` times the unmodified reference (accusim, installed under baseline/_ref) on this host's
+cores (all of them, one process each) for the same metric.
 """
 from __future__ import annotations
 
@@ -116,53 +119,86 @@ def measured_peaks():
         return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
 
 
-def cpu_baseline_port(steps_budget_s=15.0):
-    """The oracle (NumPy restatement of the reference path) on a 32,000-atom sample of the same fluid, 1 core."""
-    import numpy as np
+def reference_package():
+    """accusim, the unmodified reference (pure Python), from the repository's offline install under
+    baseline/_ref (baseline/install_reference.sh) or the environment."""
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if os.path.isdir(os.path.join(ref, "accusim")) and ref not in sys.path:
+        sys.path.insert(0, ref)
+    import accusim
+    return accusim
 
-    from devinproj_b200 import configs
-    from oracle import accusim_port as port
-    s, lj = configs.lj_fluid(20, seed=0)
-    st = port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
-                    [("Ar", configs.AR_MASS, 0.0)])
-    run = port.Run(st, [port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)],
-                   0.005 * configs.AR_TAU)
-    run.run(1)
+
+def reference_lj_fluid(accusim, n_cells, seed=0, rho_star=0.8442, T_star=0.72):
+    """The benchmark's LJ fluid built with accusim's own API only (no code of this repository): argon fcc
+    n_cells^3 (basis of examples/rahman_argon.py:23-27), rho* 0.8442, Maxwell-Boltzmann at T* with
+    default_rng(seed), LennardJones cutoff 2.5 skin 0.3, VelocityVerlet at dt* 0.005. The same state as
+    devinproj_b200.configs.lj_fluid builds."""
+    import numpy as np
+    sig, eps_k, m = 3.4e-10, 120.0, accusim.Q(39.948, "u").value
+    n = 4 * n_cells ** 3
+    L = (n / rho_star) ** (1 / 3) * sig
+    s = accusim.System(3, box=L, periodic=True)
+    s.add_species("Ar", m)
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) + 0.25
+    g = np.stack(np.meshgrid(*[np.arange(n_cells)] * 3, indexing="ij"), -1).reshape(-1, 1, 3)
+    s.add("Ar", ((g + base[None]).reshape(-1, 3)) * L / n_cells)
+    s.maxwell_boltzmann(T_star * eps_k, np.random.default_rng(seed))
+    eps = eps_k * accusim.k_B.value
+    lj = accusim.LennardJones({"Ar": (eps, sig)}, cutoff=2.5, skin=0.3)
+    tau = sig * math.sqrt(m / eps)
+    return accusim.Simulation(s, [lj], integrator=accusim.VelocityVerlet(), dt=0.005 * tau)
+
+
+def _reference_seconds_per_atom_step():
+    """The reference's NumPy cost per atom-step on this host, from 2 steps of a 2,048-atom sample (one core)."""
+    accusim = reference_package()
+    sim = reference_lj_fluid(accusim, 8, seed=1)
+    sim.run(steps=1, record_every=10 ** 9, positions=False)
     t0 = time.perf_counter()
-    run.run(1)
+    sim.run(steps=2, record_every=10 ** 9, positions=False)
+    return (time.perf_counter() - t0) / (2 * sim.system.n)
+
+
+def cpu_baseline_reference(budget_s=15.0):
+    """The unmodified reference (accusim's Simulation.run, NumPy FP64, one core) on a 32,000-atom sample of the
+    same fluid, timed after one warm-up step."""
+    accusim = reference_package()
+    sim = reference_lj_fluid(accusim, 20, seed=0)
+    sim.run(steps=1, record_every=10 ** 9, positions=False)
+    t0 = time.perf_counter()
+    sim.run(steps=1, record_every=10 ** 9, positions=False)
     t1 = time.perf_counter() - t0
-    m = int(max(3, min(60, steps_budget_s / max(t1, 1e-3))))
+    m = int(max(3, min(60, budget_s / max(t1, 1e-3))))
     t0 = time.perf_counter()
-    run.run(m)
+    sim.run(steps=m, record_every=10 ** 9, positions=False)
     dt = time.perf_counter() - t0
-    return {"value": s.n * m / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"oracle NumPy FP64 port, 32000-atom fcc 20^3 at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, "
-                      f"{m} steps after 2 warm-up steps, 1 process"}
+    return {"value": sim.system.n * m / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"accusim (unmodified, baseline/_ref) Simulation.run, NumPy FP64 cell/Verlet list, 32000-atom "
+                      f"fcc 20^3 at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, {m} steps after 2 warm-up steps, 1 process; "
+                      f"the per-atom-step cost is nearly size-independent (8.4e4 atom-steps/s at 32k, 7.9e4 at 1M "
+                      f"measured on one core)"}
 
 
 def _ref_worker(args):
     nc, steps, warmup, seed = args
-    import numpy as np  # noqa: F401
-
-    from devinproj_b200 import configs
-    from oracle import accusim_port as port
-    s, _ = configs.lj_fluid(nc, seed=seed)
-    st = port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
-                    [("Ar", configs.AR_MASS, 0.0)])
-    run = port.Run(st, [port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)],
-                   0.005 * configs.AR_TAU)
-    run.run(max(warmup, 1), record_every=10 ** 9)
+    accusim = reference_package()
+    sim = reference_lj_fluid(accusim, nc, seed=seed)
+    sim.run(steps=max(warmup, 1), record_every=10 ** 9, positions=False)
     t0 = time.perf_counter()
-    run.run(steps, record_every=10 ** 9)
-    return s.n * steps, time.perf_counter() - t0
+    sim.run(steps=steps, record_every=10 ** 9, positions=False)
+    return sim.system.n * steps, time.perf_counter() - t0
 
 
 def reference_arm(args, cfg):
-    """The reference's CPU path (the oracle port: the reference is Python and cannot travel) on all host
-    cores: one process per core, each an independent bounded sample of the workload."""
+    """The reference's own CPU path (accusim from baseline/_ref, unmodified, through Simulation.run) on all host
+    cores: one process per core, each an independent fcc sample of the workload's fluid sized so that the
+    --warmup + --steps steps take about 150 s. The NumPy cost per atom-step hardly depends on the size (8.4e4 vs
+    7.9e4 atom-steps/s at 32k and 1M atoms on one core), so the summed atom-steps/s of the samples stand for the
+    full-size run, which the reference cannot run 16 times at once (27 GB and 13 s per step each)."""
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    per_atom_step_s = 11e-6   # measured NumPy cell-list cost per atom-step on this class of host
+    per_atom_step_s = _reference_seconds_per_atom_step()
     budget = 150.0
     n_target = budget / max(args.steps + args.warmup, 1) / per_atom_step_s
     nc = int(max(4, min(20, math.floor((n_target / 4) ** (1 / 3)))))
@@ -174,14 +210,15 @@ def reference_arm(args, cfg):
     work = sum(r[0] for r in res)
     span = max(r[1] for r in res)
     value = work / span
-    sample = (f"oracle NumPy FP64 port of the reference path, {cores} processes x fcc {nc}^3 "
-              f"({4 * nc ** 3} atoms) at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, {args.steps} timed steps "
-              f"after {args.warmup} warm-up (wall {wall:.0f} s)")
+    sample = (f"accusim (unmodified reference from baseline/_ref) Simulation.run, NumPy FP64, {cores} processes x "
+              f"fcc {nc}^3 ({4 * nc ** 3} atoms, sized from a measured {per_atom_step_s * 1e6:.1f} us per atom-step) "
+              f"at rho* 0.8442 T* 0.72, rc 2.5 skin 0.3, {args.steps} timed steps after {args.warmup} warm-up "
+              f"(wall {wall:.0f} s); atom-steps/s of independent samples of the workload's fluid, summed")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * span / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -216,6 +253,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--record-every", type=int, default=100)
+    ap.add_argument("--drift-steps", type=int, default=None,
+                    help="length of the energy-drift window run after the timed region (default 10000; 2000 for the "
+                         "ensemble; 0 skips it)")
+    ap.add_argument("--fp64-steps", type=int, default=30,
+                    help="steps of the plain FP64 plug-ins (device-resident GpuSystem in accusim's Simulation.run) "
+                         "timed for the speed-up denominator; 0 skips them")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
@@ -229,6 +272,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.tpa not in (None, "auto"):
         args.tpa = int(args.tpa)
+    if args.drift_steps is None:
+        args.drift_steps = 2000 if args.workload == "ensemble" else 10000
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -252,17 +297,24 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    from devinproj_b200 import _lib
     from devinproj_b200.engine import ACC, LEN, VEL, start_engine
 
-    s, forces, dt, cfg = workload(args.workload, seed=rank)
+    ensemble = args.workload == "ensemble"
+    # the replica ensemble is one workload sharded over the ranks (largest replica first to the least-loaded
+    # rank, no collective while stepping); the single-system workloads run one independent copy per rank
+    s, forces, dt, cfg = workload(args.workload, seed=0 if ensemble else rank)
     systems, dts = (s, dt) if isinstance(s, list) else ([s], [dt])
-    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=max(args.steps // args.record_every + 2, 4),
-                                  tpa=args.tpa)
+    n_global = sum(x.n for x in systems)
+    shard = list(range(len(systems)))
+    if ensemble and world > 1:
+        from devinproj_b200.sharding import shard_replicas
+        shard = shard_replicas([x.n for x in systems], world)[rank]
+        systems, dts = [systems[r] for r in shard], [dts[r] for r in shard]
+    rec_cap = max(args.steps // args.record_every + 2, args.drift_steps // args.record_every + 2, 4)
+    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=rec_cap, tpa=args.tpa)
     n = sum(x.n for x in systems)
     pairs_lj, pairs_dsf = eng.count_pairs()
     step_blocks, coop_blocks, slots = eng.launch_info()
-    init = eng.records(1)[0, 0].copy()
     stream = torch.cuda.current_stream()
     if args.profile:
         eng.run(args.warmup, 0, True)
@@ -287,6 +339,13 @@ def main():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
     # ---------------------------------------------------------------- timed region (device events)
     eng.run(args.steps, args.record_every, True)   # instantiate the graph outside the timed region
     torch.cuda.synchronize()
@@ -304,33 +363,25 @@ def main():
         torch.cuda.synchronize()
         barrier()
         wall = time.perf_counter() - w0
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1))
     st = eng.check("timed run")
     nrec = args.steps // args.record_every + (1 if args.steps % args.record_every else 0)
     recs_all = eng.records(nrec)                     # (records, replicas, 8), engine units
     rebuilds_timed = st.rebuilds - rb0
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * args.steps * world / (ms / 1e3)
+    # weak scaling: every rank advances its own copy; the ensemble: the ranks share one fixed set of replicas
+    total_atoms = n_global if ensemble else n * world
+    value = total_atoms * args.steps / (ms / 1e3)
 
-    # energy / momentum over the timed run (the report's metrics), worst replica
+    # momentum over the timed run (the report's metric), worst replica
     pos_d, vel_d, acc_d = eng.get_state()
     vel_np = vel_d.cpu().numpy() * VEL
-    drift = slope_rel = mom_drift = 0.0
+    mom_drift = 0.0
     for r in range(len(systems)):
-        recs = recs_all[:, r, :]
-        E = recs[:, 0] + recs[:, 1]
-        scale = max(abs(E[0]), np.max(np.abs(recs[:, 0])), np.max(np.abs(recs[:, 1])))
-        drift = max(drift, float(np.max(np.abs(E - E[0])) / scale))
-        if len(E) > 2:
-            slope_rel = max(slope_rel, abs(float(np.polyfit(np.arange(len(E)) * args.record_every, E, 1)[0])) / scale)
         sr = systems[r]
         o0, o1 = eng.offsets[r], eng.offsets[r + 1]
         m_r = np.array([x.mass for x in sr.species])[sr.sp]
         pscale = float(np.sum(m_r[:, None] * np.abs(vel_np[o0:o1])))
-        P = recs[:, 2:5] * (1.66053906660e-27 * VEL)
+        P = recs_all[:, r, 2:5] * (1.66053906660e-27 * VEL)
         mom_drift = max(mom_drift, float(np.max(np.linalg.norm(P - P[0], axis=1)) / pscale))
 
     # ---------------------------------------------------------------- per-kernel timing (eager, events)
@@ -341,8 +392,10 @@ def main():
     # ---------------------------------------------------------------- accuracy vs the FP64 path
     # FP64 forces on the final state by the drop-in kernels (pinned to the reference to 1e-12); the largest
     # replica when there are several
+    pos_d, vel_d, acc_d = eng.get_state()
+    vel_np = vel_d.cpu().numpy() * VEL
     r_chk = int(np.argmax([x.n for x in systems]))
-    sr = systems[r_chk]
+    sr = systems[r_chk].copy()
     o0, o1 = eng.offsets[r_chk], eng.offsets[r_chk + 1]
     sr.pos = pos_d.cpu().numpy()[o0:o1] * LEN
     sr.vel = vel_np[o0:o1]
@@ -353,6 +406,34 @@ def main():
         Fi, _ = f.compute(sr)
         F64 += Fi
     f_err = float(np.sqrt(np.mean(np.sum((F32 - F64) ** 2, 1)) / np.mean(np.sum(F64 ** 2, 1))))
+
+    # ---------------------------------------------------------------- energy drift over a fixed window
+    # the report's metric max|E - E0| / max(|E0|, max|KE|, max|PE|) (accusim/accuracy.py:70-76) over
+    # --drift-steps steps from the current state, E recorded at the window's start and every record_every steps
+    drift = slope_rel = None
+    drift_ms = None
+    if args.drift_steps > 0:
+        eng.run(1, 0, True)                      # the window starts from a recorded state
+        start = eng.records(1)[0].copy()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        eng.run(args.drift_steps, args.record_every, True)
+        d1.record(stream)
+        torch.cuda.synchronize()
+        eng.check("drift window")
+        drift_ms = d0.elapsed_time(d1)
+        nrec_d = args.drift_steps // args.record_every + (1 if args.drift_steps % args.record_every else 0)
+        recs = np.concatenate([start[None], eng.records(nrec_d)])          # (1 + records, replicas, 8)
+        steps_at = np.concatenate([[0], np.minimum(np.arange(1, nrec_d + 1) * args.record_every, args.drift_steps)])
+        drift = slope_rel = 0.0
+        for r in range(len(systems)):
+            KE, PE = recs[:, r, 0], recs[:, r, 1]
+            E = KE + PE
+            scale = max(abs(E[0]), np.max(np.abs(KE)), np.max(np.abs(PE)))
+            drift = max(drift, float(np.max(np.abs(E - E[0])) / scale))
+            slope_rel = max(slope_rel, abs(float(np.polyfit(steps_at, E, 1)[0])) / scale)
+        drift = max_over_ranks(drift)
+        slope_rel = max_over_ranks(slope_rel)
 
     # ---------------------------------------------------------------- end to end (host buffers)
     pos_h = (pos_d.cpu() * 1.0).pin_memory()
@@ -378,13 +459,16 @@ def main():
         vel_h, out_v = out_v, vel_h
     torch.cuda.synchronize()
     barrier()
-    e2e_s = time.perf_counter() - w0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_val = n * args.e2e_steps * world / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - w0)
+    e2e_val = total_atoms * args.e2e_steps / e2e_s
     eng.check("e2e")
+    del rec
+
+    # ---------------------------------------------------------------- the plain FP64 GPU drop-in
+    fp64 = None
+    if args.fp64_steps > 0 and not ensemble:
+        fp64 = fp64_dropin_device_resident(args, local, stream)
+    del eng
 
     peaks, peak_kind = measured_peaks()
     clocks = clk.summary()
@@ -405,13 +489,18 @@ def main():
     launches = 2 + 2 * args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if ensemble and world > 1 else "weak",
         "vs_baseline": None, "dtype": "fp32-pairs/f64-state", "data": "synthetic (seeded fcc lattice, MB velocities)",
         "config": full_config(cfg, args, world),
-        "accuracy": {"force_rms_rel_err_vs_fp64": f_err, "energy_drift_report_metric": drift,
-                     "drift_note": "max over replicas" if len(systems) > 1 else "single system",
-                     "energy_drift_per_step_rel": slope_rel,
-                     "momentum_drift_report_metric": mom_drift, "steps_in_drift_window": args.steps,
+        "accuracy": {"force_rms_rel_err_vs_fp64": f_err,
+                     "energy_drift_report_metric": drift, "energy_drift_window_steps": args.drift_steps,
+                     "energy_drift_linear_per_step_rel": slope_rel, "energy_drift_window_ms": drift_ms,
+                     "drift_note": ("report metric max|E-E0|/scale over a fixed window after the timed region, E "
+                                    f"recorded at its start and every {args.record_every} steps; "
+                                    + ("max over replicas and ranks" if len(systems) > 1 or world > 1
+                                       else "single system")),
+                     "momentum_drift_report_metric": mom_drift, "momentum_window_steps": args.steps,
                      "rebuilds_in_timed_region": int(rebuilds_timed)},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": traffic, "kernel": "k_step",
@@ -428,13 +517,64 @@ def main():
         "gpu_launches": launches,
         "wall_s_timed": wall,
     }
+    if ensemble:
+        line["sharding"] = {"replicas": len(shard) if world == 1 else None, "replicas_total": 768,
+                            "this_rank_replicas": len(shard), "this_rank_atoms": n, "atoms_total": n_global,
+                            "rule": "largest replica first to the least-loaded rank; no collective while stepping"}
+    if fp64 is not None:
+        fp64["fp32c_over_fp64"] = (value / world) / fp64["value"]
+        line["fp64_dropin_device_resident"] = fp64
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_port()
+        line["cpu_baseline"] = cpu_baseline_reference()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp64_dropin_device_resident(args, local, stream):
+    """Throughput of the plain FP64 GPU plug-ins (LennardJones / DampedShiftedCoulomb / VelocityVerlet) inside
+    accusim's own Simulation.run on a device-resident GpuSystem of the same workload: per step the FP64 kick,
+    drift and wrap kernels, the FP64 pair kernel over the device Verlet list (rebuilt on the device when the
+    skin test fires), the closing kick, and the potential-energy read-back that accusim's Simulation contract
+    needs every step; the state crosses PCIe only at records (one at the end of the timed call). Timed with
+    CUDA events and the wall clock around one Simulation.run call, SM clocks sampled."""
+    import torch
+
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, VelocityVerlet
+    from devinproj_b200._accusim import simulation as _asim
+    s, forces, dt, _ = workload(args.workload, seed=0)
+    from devinproj_b200 import GpuSystem
+    g = GpuSystem.from_system(s)
+    fresh = []
+    for f in forces:   # plug-ins of their own (a Verlet list per force object)
+        if isinstance(f, LennardJones):
+            fresh.append(LennardJones(f.params, cutoff=f.cutoff, pairlist_threshold=f.pairlist_threshold, skin=f.skin))
+        elif isinstance(f, DampedShiftedCoulomb):
+            fresh.append(DampedShiftedCoulomb(f.rcut, alpha=f.alpha, k=f.k, pairlist_threshold=f.pairlist_threshold,
+                                              exclude=f.exclude, skin=f.skin))
+    sim = _asim.Simulation(g, fresh, integrator=VelocityVerlet(), dt=dt)
+    sim.run(steps=3, record_every=10 ** 9, positions=False)          # warm-up (and the first upload)
+    torch.cuda.synchronize()
+    rb0 = fresh[0].rebuilds
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.2)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(stream)
+        sim.run(steps=args.fp64_steps, record_every=10 ** 9, positions=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+    ms = e0.elapsed_time(e1)
+    return {"value": g.n * args.fp64_steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.fp64_steps,
+            "steps": args.fp64_steps, "wall_s": wall, "list_rebuilds": fresh[0].rebuilds - rb0,
+            "path": "accusim.Simulation.run (unmodified, baseline/_ref) + devinproj_b200.GpuSystem (state resident on "
+                    "the GPU) + FP64 LennardJones/DampedShiftedCoulomb/VelocityVerlet plug-ins; host sync of the "
+                    "potential energy each step (accusim's contract), state at the final record only",
+            "dtype": "f64", "clocks": clk.summary()}
 
 
 WORKLOADS = {
@@ -550,20 +690,27 @@ def run_experiment(args):
                           "energy_drift_report_metric": drift, "linear_drift_per_step_rel": slope,
                           "ms_per_step": e0.elapsed_time(e1) / steps, "rebuilds": eng.status().rebuilds}), flush=True)
     elif args.experiment == "dropin":
-        from devinproj_b200 import Simulation, VelocityVerlet
-        s, forces, dt, cfg = workload(args.workload, seed=0)
-        sim = Simulation(s, forces, integrator=VelocityVerlet(), dt=dt)
-        sim.run(steps=2, record_every=10 ** 9, positions=False)
-        torch.cuda.synchronize()
-        n = 5
-        t0 = time.perf_counter()
-        sim.run(steps=n, record_every=10 ** 9, positions=False)
-        torch.cuda.synchronize()
-        dt_s = time.perf_counter() - t0
-        print(json.dumps({"experiment": "fp64_dropin_throughput", "workload": cfg["workload"], "steps": n,
-                          "atom_steps_per_s": s.n * n / dt_s, "ms_per_step": 1e3 * dt_s / n,
-                          "path": "Simulation.run with the FP64 drop-in VelocityVerlet and forces (host state, "
-                                  "per-step H2D/D2H)"}), flush=True)
+        # the FP64 plug-ins inside accusim's Simulation.run: on a device-resident GpuSystem (the honest FP64 GPU
+        # figure) and on accusim's plain System (state copied to and from the host every step)
+        from devinproj_b200 import VelocityVerlet
+        from devinproj_b200._accusim import simulation as _asim
+        from devinproj_b200.state import GpuSystem
+        out = {}
+        for kind in ("device_resident", "host_round_trip"):
+            s, forces, dt, cfg = workload(args.workload, seed=0)
+            if kind == "device_resident":
+                s = GpuSystem.from_system(s)
+            sim = _asim.Simulation(s, forces, integrator=VelocityVerlet(), dt=dt)
+            sim.run(steps=3, record_every=10 ** 9, positions=False)
+            torch.cuda.synchronize()
+            n = max(args.steps, 5) if kind == "device_resident" else 5
+            t0 = time.perf_counter()
+            sim.run(steps=n, record_every=10 ** 9, positions=False)
+            torch.cuda.synchronize()
+            dt_s = time.perf_counter() - t0
+            out[kind] = {"steps": n, "atom_steps_per_s": s.n * n / dt_s, "ms_per_step": 1e3 * dt_s / n}
+        print(json.dumps({"experiment": "fp64_dropin_throughput", "workload": cfg["workload"], **out,
+                          "path": "accusim.Simulation.run with the FP64 VelocityVerlet and force plug-ins"}), flush=True)
 
 
 def workload_meta(name):

@@ -19,12 +19,38 @@ CACHE = os.environ.get("ACS_AUTOTUNE_CACHE", os.path.join(os.path.expanduser("~"
                                                           "autotune.json"))
 
 
-def signature(systems, rlist):
+def forcefield_tag(forces):
+    """The force terms a workload evaluates (they change the pair kernel's cost per entry): lj, dsf, and dsf with
+    exclusions."""
+    from ._accusim import forces as _af
+    tags = []
+    for f in forces:
+        if isinstance(f, _af.LennardJones):
+            tags.append("lj")
+        elif isinstance(f, _af.DampedShiftedCoulomb):
+            tags.append("dsfx" if f.exclude else "dsf")
+    return "+".join(sorted(tags))
+
+
+def device_tag():
+    """The GPU the timings were taken on (a tuned launch shape is not carried over to another model)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name().replace(" ", "-")
+    except Exception:
+        pass
+    return "nodevice"
+
+
+def signature(systems, rlist, forces=(), device=None):
     n = sum(s.n for s in systems)
     vol = sum(float(np.prod(s.box)) for s in systems)
     rho_nb = n / vol * 4.0 / 3.0 * math.pi * rlist ** 3     # neighbours per atom inside the list radius
     bucket = lambda x: float(f"{x:.2g}")                    # noqa: E731
-    return f"n{bucket(n)}_r{len(systems)}_nb{bucket(rho_nb)}_sp{len(systems[0].species)}"
+    dev = device if device is not None else device_tag()
+    return (f"n{bucket(n)}_r{len(systems)}_nb{bucket(rho_nb)}_sp{len(systems[0].species)}"
+            f"_ff{forcefield_tag(forces) or 'none'}_{dev}")
 
 
 def _load():
@@ -57,7 +83,7 @@ def tune(systems, forces, dts, steps=30, use_cache=True, verbose=False):
     """Best (tpa, grid_mult) for these replicas. Runs the engine a few steps per candidate on the GPU."""
     from .engine import forcefield_from, start_engine
     _, rlist, _ = forcefield_from(forces, systems[0].species)
-    key = signature(systems, rlist)
+    key = signature(systems, rlist, forces)
     db = _load() if use_cache else {}
     if key in db:
         return tuple(db[key]["best"])

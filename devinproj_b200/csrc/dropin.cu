@@ -139,20 +139,18 @@ __global__ void k_scatter(const int32_t* __restrict__ cell_of, int64_t n, const 
   cell_atoms[start[c] + slot] = (int32_t)i;
 }
 
-// Atoms of a cell in ascending index order, so list order is deterministic run to run.
-__global__ void k_sort_cells(const int32_t* __restrict__ start, int64_t ncells, int32_t* __restrict__ cell_atoms) {
-  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
-  int s = start[c], e = start[c + 1];
-  for (int a = s + 1; a < e; ++a) {
-    int v = cell_atoms[a];
-    int b = a - 1;
-    while (b >= s && cell_atoms[b] > v) {
-      cell_atoms[b + 1] = cell_atoms[b];
-      --b;
-    }
-    cell_atoms[b + 1] = v;
-  }
+// Atoms of a cell in ascending index order, so list order is deterministic run to run: every atom's rank among
+// its cell's atoms (the scatter's arbitrary order in `unsorted`) gives its place. A thread per atom; the reads
+// of a cell's members are shared by the cell's atoms through L1.
+__global__ void k_rank_cells(const int32_t* __restrict__ cell_of, int64_t n, const int32_t* __restrict__ start,
+                             const int32_t* __restrict__ unsorted, int32_t* __restrict__ cell_atoms) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = cell_of[i];
+  const int s = start[c], e = start[c + 1];
+  int rank = 0;
+  for (int b = s; b < e; ++b) rank += unsorted[b] < (int32_t)i;
+  cell_atoms[s + rank] = (int32_t)i;
 }
 
 __device__ __forceinline__ void stencil_range(int c, int nc, int periodic, int& lo, int& hi) {
@@ -491,6 +489,7 @@ int bin_cells(const double* pos, int64_t n, const acs_grid* g, void* work, cudaS
   int32_t* count = (int32_t*)w; w += align256((nc + 1) * 4);
   cb.start = (int32_t*)w; w += align256((nc + 1) * 4);
   cb.cell_atoms = (int32_t*)w; w += align256(n * 4);
+  int32_t* unsorted = (int32_t*)w; w += align256(n * 4);
   int32_t* sums = (int32_t*)w;
   GridDev gd = to_dev(g);
   if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return 1;
@@ -500,8 +499,8 @@ int bin_cells(const double* pos, int64_t n, const acs_grid* g, void* work, cudaS
   k_scan_sums<<<1, kScanThreads, 0, s>>>(sums, nchunks, nullptr);
   k_scan_add<<<(int)nchunks, 256, 0, s>>>(cb.start, nc + 1, sums);
   if (cudaMemsetAsync(count, 0, (nc + 1) * 4, s) != cudaSuccess) return 1;
-  k_scatter<<<nb, kBlock, 0, s>>>(cb.cell_of, n, cb.start, count, cb.cell_atoms);
-  k_sort_cells<<<(int)ceil_div(nc, kBlock), kBlock, 0, s>>>(cb.start, nc, cb.cell_atoms);
+  k_scatter<<<nb, kBlock, 0, s>>>(cb.cell_of, n, cb.start, count, unsorted);
+  k_rank_cells<<<nb, kBlock, 0, s>>>(cb.cell_of, n, cb.start, unsorted, cb.cell_atoms);
   return 0;
 }
 
@@ -570,7 +569,7 @@ size_t acs_nlist_work_bytes(int64_t n, const acs_grid* g) {
   if (!g || n < 0) return 0;
   const int64_t nc = grid_cells(g);
   const int64_t nchunks = ceil_div(nc + 1, kScanChunk);
-  return align256(n * 4) + 2 * align256((nc + 1) * 4) + align256(n * 4) + align256((nchunks + 1) * 4);
+  return align256(n * 4) + 2 * align256((nc + 1) * 4) + 2 * align256(n * 4) + align256((nchunks + 1) * 4);
 }
 
 int acs_nlist_build(const double* pos, int64_t n, const acs_grid* g, int32_t maxnb, int32_t* nbr, int32_t* nnb,
@@ -775,21 +774,55 @@ constexpr int64_t kNoAllocMaxBlocks = 8192;                   // 8192 partials o
 constexpr int64_t kNoAllocMaxAtoms = kNoAllocMaxBlocks * kBlock;  // 2,097,152
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocMaxBlocks * 8 + 256];
 
-constexpr int kMaxDevices = 64;
+// The address is looked up once per CUDA context (the primary context of each device, or any context a driver-API
+// caller makes current): a symbol's address belongs to the context the module was loaded into, so a cache keyed
+// by the device alone would hand a non-primary context, or a primary context re-created after cudaDeviceReset,
+// an address it cannot use.
+struct NoAllocEntry {
+  int dev;
+  void* ctx;
+  void* ptr;
+};
+constexpr int kNoAllocCache = 64;
 std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+NoAllocEntry g_noalloc_cache[kNoAllocCache];
+int g_noalloc_used = 0;
 
-// Device address of g_noalloc_scratch on the current device, looked up on the first call per device.
+// cuCtxGetCurrent through the runtime's driver entry point (no link against libcuda); null if unavailable.
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (CtxGetCurrentFn)p;
+  }();
+  return fn;
+}
+
+// Device address of g_noalloc_scratch in the current context, looked up on the first call in that context.
+// Before the runtime has made a context current, the symbol lookup itself initialises the device's primary
+// context, which is then the current one.
 int noalloc_scratch(void** out) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ACS_ERR_NO_DEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return ACS_ERR_NO_DEVICE;
+  CtxGetCurrentFn get = ctx_get_current();
+  void* ctx = nullptr;
+  if (!get || get(&ctx) != 0) return ACS_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ACS_ERR_CUDA;
-    g_noalloc_ptr[dev] = p;
+  for (int k = 0; ctx && k < g_noalloc_used; ++k) {
+    if (g_noalloc_cache[k].dev == dev && g_noalloc_cache[k].ctx == ctx) {
+      *out = g_noalloc_cache[k].ptr;
+      return ACS_OK;
+    }
   }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ACS_ERR_CUDA;
+  if (!ctx && (get(&ctx) != 0 || !ctx)) return ACS_ERR_CUDA;
+  if (g_noalloc_used < kNoAllocCache) g_noalloc_cache[g_noalloc_used++] = NoAllocEntry{dev, ctx, p};
+  *out = p;
   return ACS_OK;
 }
 

@@ -41,7 +41,7 @@ constexpr int kCellChunk = 1024;  // cell-scan chunk (4 cells per thread of a 25
 constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
-constexpr long long kSpinLimit = 20000000;  // ~2 s of 100 ns sleeps
+constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
 
 struct RepDev {
   int64_t atom0;
@@ -119,6 +119,7 @@ struct Eng {
   uint32_t jmask;                // slot bits of a list entry: 26 with exclusions, else 27
   uint32_t seed_lo, seed_hi;
   unsigned long long* octr;      // O-steps taken so far (Langevin draws: counter)
+  long long spin_limit;          // polls of a grid-barrier wait before it gives up (0: give up at once)
 };
 
 // ------------------------------------------------------------------- Langevin normal draws --
@@ -216,7 +217,9 @@ __device__ __forceinline__ void cell_coords(int local, const RepDev& R, int& c0,
 }
 
 // ------------------------------------------------------------------------ bounded grid barrier --
-__device__ bool grid_sync(unsigned int* bar, acs_dev_status* st) {
+// A block that is not the last to arrive polls the generation word up to `limit` times (100 ns apart); if the
+// barrier has not opened by then it sets ACS_FLAG_TIMEOUT and returns false, and the caller's kernel returns.
+__device__ bool grid_sync(unsigned int* bar, acs_dev_status* st, long long limit) {
   __syncthreads();
   __shared__ int ok;
   if (threadIdx.x == 0) {
@@ -232,7 +235,7 @@ __device__ bool grid_sync(unsigned int* bar, acs_dev_status* st) {
     } else {
       long long it = 0;
       while (*vgen == gen) {
-        if (++it > kSpinLimit) {
+        if (it++ >= limit) {
           atomicOr(&st->flags, ACS_FLAG_TIMEOUT);
           ok = 0;
           break;
@@ -863,7 +866,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         E.chunk_part[(int64_t)c * kRecW + threadIdx.x] = s;
       }
     }
-    if (!grid_sync(E.bar, E.status)) return;
+    if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
     // Q2: per-replica sum of its chunks in order
     for (int r = blockIdx.x; r < E.R; r += gridDim.x) {
       if (!E.active[r] || threadIdx.x >= kRecW) continue;
@@ -903,7 +906,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     atomicAdd(&E.phase_ns[k], t_now - t_prev);                    \
     t_prev = t_now;                                               \
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(1);
 
   // P0: clear counters of flagged replicas' cells
@@ -913,7 +916,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       E.cursor[c] = 0;
     }
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(2);
   // P1: absolute wrapped positions and new cells
   for (int64_t s = gtid; s < E.S; s += gstride) {
@@ -944,7 +947,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     E.newcell[s] = c;
     atomicAdd(&E.count[c], 1);
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(3);
   // P2: exclusive scan of cell counts -> slot starts, in fixed 1024-cell chunks: (a) chunk-local scans,
   // (b) per-replica prefix of chunk totals (also: sentinel, clear flag, count the rebuild), (c) offsets.
@@ -968,7 +971,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     }
     if (threadIdx.x == 0) E.cc_sum[c] = total;
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(4);
   for (int64_t r = gtid; r < E.R; r += gstride) {
     if (!fl[r]) continue;
@@ -983,14 +986,14 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     E.flag[r] = 0;
     atomicAdd(&E.status->rebuilds, 1);
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(5);
   for (int c = blockIdx.x; c < E.ncc; c += gridDim.x) {
     if (!fl[E.cc_rep[c]]) continue;
     const int c0 = E.cc_c0[c], nc = E.cc_n[c], add_v = E.cc_sum[c];
     for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) E.start[c0 + idx] += add_v;
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(6);
   // P3: scatter old slots to new slots
   for (int64_t s = gtid; s < E.S; s += gstride) {
@@ -999,7 +1002,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     const int c = E.newcell[s];
     E.perm[E.start[c] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(7);
   // P3b: deterministic order inside each cell: every atom's rank among its cell's atoms by old slot
   for (int64_t k = gtid; k < E.S; k += gstride) {
@@ -1012,7 +1015,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     for (int a = a0; a < a1; ++a) rank += (E.perm[a] < v);
     E.perm2[a0 + rank] = v;
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(8);
   // P4: gather into new order
   for (int64_t k = gtid; k < E.S; k += gstride) {
@@ -1028,7 +1031,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       E.tmp_v[3 * k + d] = E.v[3 * o + d];
     }
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(9);
   // P5: commit; offsets from the new cell origins; images
   for (int64_t k = gtid; k < E.S; k += gstride) {
@@ -1055,7 +1058,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     for (int d = 0; d < 3; ++d) E.v[3 * k + d] = E.tmp_v[3 * k + d];
     E.img[dst][k] = make_img(ux, uy, uz, E.tmp_sp[k]);
   }
-  if (!grid_sync(E.bar, E.status)) return;
+  if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(10);
   // P6: neighbour lists in one pass over the 27-cell stencil. Each candidate's r^2 is first computed in
   // FP32 from the new images (relative error ~1e-6): outside rl^2 (1 + 1e-4) it is rejected, inside
@@ -1419,6 +1422,35 @@ __global__ void k_count_pairs(Eng E, FFDev ff, int src, unsigned long long* out)
   atomicAdd(out + 1, nd);
 }
 
+// Every neighbour-list entry as a directed pair of caller indices, key = 2 (gi n_total + gj) + excluded (the DSF
+// exclusion flag of the entry), and the FP64 absolute positions the lists were built from (the last rebuild's
+// wrapped positions, which its exact pair filter used), in caller order. Each slot reserves its entries with one
+// atomic; keys beyond `cap` are counted but not written. Order is not deterministic: the caller sorts.
+__global__ void k_dump_lists(Eng E, const int64_t* __restrict__ src0, int64_t n_total, long long* __restrict__ keys,
+                             long long cap, unsigned long long* __restrict__ count, double* __restrict__ pos_build) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E.S; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = E.tile_rep[i >> 5];
+    const RepDev& R = E.rep[r];
+    if (i - R.atom0 >= R.n) continue;
+    const int64_t gi = src0[r] + E.id[i];
+    if (pos_build) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) pos_build[3 * gi + d] = E.tmp_xa[3 * i + d];
+    }
+    const int m = E.nnb[i];
+    const unsigned long long base = atomicAdd(count, (unsigned long long)m);
+    const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
+    for (int k = 0; k < m; ++k) {
+      const uint32_t e = (uint32_t)lst[(int64_t)k * E.G];
+      const int64_t j = (int64_t)(e & E.jmask);
+      const bool own = j < E.S && E.tile_rep[j >> 5] == r && j - R.atom0 < R.n;
+      const int64_t gj = own ? src0[r] + E.id[j] : -1;   // -1: an entry naming no atom of this replica
+      const long long key = gj < 0 ? -1ll : 2ll * (gi * n_total + gj) + ((e & E.ex_bit) ? 1 : 0);
+      if (base + k < (unsigned long long)cap) keys[base + k] = key;
+    }
+  }
+}
+
 // Radial descriptors of every slot from the engine's own images and neighbour lists (FP32), in slot order,
 // for the learned force correction: warp per slot, lane = Gaussian channel (definitions as in mlp.cu).
 struct DescP {
@@ -1743,6 +1775,16 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   return L;
 }
 
+// erfc_as (the FP32 DSF pair term's Abramowitz & Stegun 7.1.26 erfc) evaluated in FP64 on the host with the same
+// coefficients. The DSF shift constants come from it, so the engine's shifted potential and force vanish at rc
+// under the approximation the pair term uses (with the exact erfc there they would jump by up to 1.5e-7 q_i q_j k
+// / rc when a pair crosses the cutoff).
+double erfc_as_host(double x) {
+  const double t = 1.0 / fma(0.3275911, x, 1.0);
+  const double q = fma(t, fma(t, fma(t, fma(t, 1.061405429, -1.453152027), 1.421413741), -0.284496736), 0.254829592);
+  return t * q * exp(-x * x);
+}
+
 FFDev make_ff(const acs_forcefield& f, int& err) {
   FFDev ff{};
   err = ACS_OK;
@@ -1780,7 +1822,7 @@ FFDev make_ff(const acs_forcefield& f, int& err) {
   if (f.dsf) {
     const double a = f.dsf_alpha, rc = f.dsf_rcut;
     const double c = 2.0 * a / sqrt(M_PI);
-    const double erc = erfc(a * rc);
+    const double erc = erfc_as_host(a * rc);
     const double fshift = erc / (rc * rc) + c * exp(-(a * rc) * (a * rc)) / rc;
     ff.dsf_a = (float)a;
     ff.dsf_rc = (float)rc;
@@ -2013,6 +2055,7 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.ex_bit = cfg->n_ex_ids > 0 ? kExBit : 0u;
   E.jmask = cfg->n_ex_ids > 0 ? kExBit - 1u : kIdxMask;
   E.thermo = cfg->thermo.kind;
+  E.spin_limit = cfg->barrier_wait_limit == 0 ? kSpinLimit : (cfg->barrier_wait_limit < 0 ? 0 : cfg->barrier_wait_limit);
   E.seed_lo = (uint32_t)cfg->thermo.seed;
   E.seed_hi = (uint32_t)(cfg->thermo.seed >> 32);
 
@@ -2181,6 +2224,10 @@ int acs_engine_status(acs_engine* e, acs_dev_status* out, int clear, void* strea
     if (cudaMemcpyAsync(e->E.status, &z, sizeof(z), cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
       return ACS_ERR_CUDA;
+    // a barrier that timed out leaves its arrival count behind: start the next launch from a clean barrier
+    if ((out->flags & ACS_FLAG_TIMEOUT) &&
+        (cudaMemsetAsync(e->E.bar, 0, 16, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess))
+      return ACS_ERR_CUDA;
   }
   return ACS_OK;
 }
@@ -2227,6 +2274,17 @@ int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* str
   if (cudaMemsetAsync(out_dev, 0, 16, s) != cudaSuccess) return ACS_ERR_CUDA;
   // images of buffer 0 are current after acs_engine_set_state (and after any rebuild into buffer 0)
   k_count_pairs<<<e->step_blocks, 256, 0, s>>>(e->E, e->ff, 0, out_dev);
+  return launch_status();
+}
+
+int acs_engine_dump_lists(acs_engine* e, long long* keys_dev, long long cap, unsigned long long* count_dev,
+                          double* pos_build_dev, void* stream) {
+  if (!e || !count_dev || cap < 0 || (cap > 0 && !keys_dev)) return ACS_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(count_dev, 0, sizeof(unsigned long long), s) != cudaSuccess) return ACS_ERR_CUDA;
+  int64_t n_total = 0;
+  for (const RepDev& R : e->reps) n_total += R.n;
+  k_dump_lists<<<e->step_blocks, 256, 0, s>>>(e->E, e->src0_dev, n_total, keys_dev, cap, count_dev, pos_build_dev);
   return launch_status();
 }
 

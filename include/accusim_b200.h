@@ -117,8 +117,9 @@ int acs_lj_fp64(const double* pos, const int32_t* sp, int64_t n, const double* b
  * forbidden after start-up, or the host hands out only input/output buffers). No counterpart in the
  * reference. Same arguments and results as acs_lj_fp64 without the work buffer: the reduction scratch is a
  * 64 KiB static device array inside the library, held on every GPU that loads it until exit, so
- * n <= 2,097,152 (ACS_ERR_UNSUPPORTED above). The first call on a device looks up that array's address, so
- * make it before any stream capture. Calls share the array: calls that overlap on the GPU race. */
+ * n <= 2,097,152 (ACS_ERR_UNSUPPORTED above). The first call in each CUDA context (a device's primary context,
+ * or a context a driver-API caller made current) looks up that array's address in the context, so make it
+ * before any stream capture. Calls share the array: calls that overlap on the GPU race. */
 int acs_lj_fp64_noalloc(const double* pos, const int32_t* sp, int64_t n, const double* box3, int periodic,
                         const int32_t* nbr, const int32_t* nnb, int32_t maxnb, int32_t n_species,
                         const double* eps_tab, const double* sig_tab, double cutoff, double* force,

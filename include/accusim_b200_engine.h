@@ -76,6 +76,12 @@ typedef struct acs_engine_config {
   const int32_t* ex_ids;        /* ex_start[n_ex_ids] entries */
   int32_t n_ex_ids;
   int32_t pad2;
+  /* Grid-barrier waits of the cooperative list-maintenance kernel: a block polls up to this many times,
+   * 100 ns apart, then reports ACS_FLAG_TIMEOUT (acs_engine_status; later kernels of the engine return at
+   * once until the status is cleared, which also resets the barrier) and its kernel returns.
+   * 0: the default, 2e7 polls (~2 s); negative: no polling (a block that is not the last to arrive gives up
+   * at once, which makes the timeout path testable). */
+  int64_t barrier_wait_limit;
 } acs_engine_config;
 
 typedef struct acs_engine acs_engine;
@@ -100,6 +106,15 @@ int acs_engine_load_state(acs_engine* e, const double* pos, const double* vel, v
 /* out_dev[0] = ordered LJ pairs inside cutoff*sigma_ij, out_dev[1] = ordered DSF pairs inside rc (each
  * unordered pair counted twice), on the images set by the last acs_engine_set_state. */
 int acs_engine_count_pairs(acs_engine* e, unsigned long long* out_dev, void* stream);
+/* The engine's neighbour lists as they are, for checking them against accusim's pair search
+ * (accusim/forces.py:279-321 cell_list_pairs, accusim/forces.py:86-98 VerletList.pairs) at the list radius:
+ * every list entry as a directed pair of caller indices (global over replicas, in replica order),
+ * keys_dev[k] = 2 (i n_total + j) + excluded, excluded = the entry's DSF exclusion flag (-1 for an entry
+ * that does not name an atom of its own replica), in no particular order; *count_dev = number of entries
+ * (entries beyond cap are counted, not written). pos_build_dev (optional, n_total x 3) receives the FP64
+ * absolute positions of the last rebuild, from which the lists were built. Device arrays. */
+int acs_engine_dump_lists(acs_engine* e, long long* keys_dev, long long cap, unsigned long long* count_dev,
+                          double* pos_build_dev, void* stream);
 /* Synchronous: copies the device status block to *out (optionally clearing its error flags). */
 int acs_engine_status(acs_engine* e, acs_dev_status* out, int clear, void* stream);
 int acs_engine_neighbor_stats(acs_engine* e, int32_t* max_nnb, int64_t* sum_nnb, void* stream);

@@ -17,6 +17,15 @@ def test_signature_buckets_and_distinguishes_workloads():
     assert autotune.signature([s1], rl) != autotune.signature([s1, s2], rl)     # replica count is part of it
     assert autotune.signature([s1], rl) != autotune.signature([s1], 2 * rl)     # so is the list density
     assert autotune.signature([s1], rl).startswith("n260.0_r1_")     # 256 atoms, bucketed to 2 significant digits
+    # the force terms and the GPU model are part of it
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones
+    lj = LennardJones({"Ar": (1.6e-21, 3.4e-10)})
+    dsf = DampedShiftedCoulomb(rcut=1e-9)
+    dsfx = DampedShiftedCoulomb(rcut=1e-9, exclude=[(0, 1)])
+    keys = {autotune.signature([s1], rl, ff, device="B200") for ff in ([lj], [lj, dsf], [lj, dsfx], [dsf])}
+    assert len(keys) == 4
+    assert autotune.signature([s1], rl, [lj], device="B200") != autotune.signature([s1], rl, [lj], device="H100")
+    assert autotune.signature([s1], rl, [lj], device="B200").endswith("_fflj_B200")
 
 
 def test_candidates():
@@ -35,7 +44,7 @@ def test_cache_round_trip_and_cached_answer(tmp_path, monkeypatch):
     s, lj = configs.lj_fluid(4, seed=0)
     from devinproj_b200.engine import forcefield_from
     _, rlist, _ = forcefield_from([lj], s.species)
-    key = autotune.signature([s], rlist)
+    key = autotune.signature([s], rlist, [lj])
     autotune._store({key: {"best": [2, 0], "ms_per_step": {"1,0": 0.2, "2,0": 0.1}}})
     assert json.loads(cache.read_text())[key]["best"] == [2, 0]
     assert not (tmp_path / "sub" / "autotune.json.tmp").exists()    # written through a rename

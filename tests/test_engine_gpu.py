@@ -18,6 +18,16 @@ def rms_rel(F, Fref):
     return float(np.sqrt(np.mean(np.sum((F - Fref) ** 2, 1)) / np.mean(np.sum(Fref ** 2, 1))))
 
 
+def energy_drift(tr):
+    """The report's energy metric (the oracle's restatement of accusim/accuracy.py:70-76) of a trajectory."""
+    return port.energy_drift(np.array(tr.total_energy), np.array(tr.kinetic), np.array(tr.potential))
+
+
+def momentum_drift(tr, s):
+    """The report's momentum metric (the oracle's restatement of accusim/accuracy.py:86-91)."""
+    return port.momentum_drift(np.array(tr.momentum), s.masses, s.vel)
+
+
 def oracle_of(s):
     return port.State(s.pos.copy(), s.vel.copy(), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
                       [(x.name, x.mass, x.charge) for x in s.species])
@@ -111,7 +121,8 @@ def test_engine_lj_species_without_parameters_do_not_interact():
     interaction, and the list radius uses sigma_max over interacting pairs only. A 2048-atom Ar/Kr/tracer
     mixture (a third of the atoms a tracer species with no parameters), engine vs the FP64 plug-in, at the
     start and after 100 steps."""
-    from devinproj_b200 import GpuSimulation, LennardJones, System, configs
+    from accusim import System
+    from devinproj_b200 import GpuSimulation, LennardJones, configs
     rng = np.random.default_rng(9)
     base, _ = configs.lj_fluid(8, seed=9)
     s = System(3, box=base.box.copy(), periodic=True)
@@ -142,7 +153,8 @@ def test_engine_orthorhombic_boxes(nz, tpa):
     """Boxes with unequal edges: an LJ fluid on a perturbed 28 x 19 x nz lattice (spacing 1.06 sigma; box 29.7
     x 20.1 x 6.4 sigma has a one-cell axis, 12.7 sigma does not), engine vs the FP64 plug-in at the start and
     after 100 steps, through the thread-per-atom (one-cell axis), warp-per-atom and warp-per-cell list builds."""
-    from devinproj_b200 import GpuSimulation, LennardJones, System, configs
+    from accusim import System
+    from devinproj_b200 import GpuSimulation, LennardJones, configs
     rng = np.random.default_rng(nz + tpa)
     a = 1.06 * configs.AR_SIGMA
     n = np.array([28, 19, nz])
@@ -169,7 +181,6 @@ def test_engine_box_smaller_than_twice_the_list_radius(golden):
     plug-in at the start and after 100 steps, one rebuild per step, and the energy drift of the 100 steps no
     more than 10x the reference's over its 60-step run of the undisplaced lattice."""
     from devinproj_b200 import GpuSimulation, LennardJones
-    from devinproj_b200.accuracy import energy_drift
     g = golden("report_argon108")
     s = product_system(g)
     assert 2 * 2.8 * float(g["sig"]) > s.box[0]
@@ -216,7 +227,6 @@ def test_gpu_simulation_report_matches_reference_rows(golden):
 def test_engine_trajectory_tracks_reference_and_conserves(golden):
     """60 steps of the 864-atom argon case: energy series against the reference's FP64 run."""
     from devinproj_b200 import GpuSimulation, LennardJones
-    from devinproj_b200.accuracy import energy_drift, momentum_drift
     g = golden("argon864")
     s = product_system(g, "0")
     sim = GpuSimulation(s, [LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)],
@@ -264,20 +274,29 @@ def test_engine_lists_stay_valid_across_rebuilds():
 def test_engine_full_size_lj1m_pair_set_forces_and_net_force():
     """The headline system at full size (1,048,576-atom LJ fluid, fcc 64^3, rho* 0.8442, T* 0.72), through
     size-independent properties, on the displaced lattice and again on the state after 200 steps (about 20
-    rebuilds): the engine's lists hold exactly twice the FP64 pair set at the list radius (the drop-in's
-    cell_list_pairs, itself pinned to the reference's pair sets); FP32c forces within the force tolerance of
-    the FP64 plug-in's on the same positions, energy within 2e-6, and the net force at round-off."""
+    rebuilds): the engine's lists, decoded entry by entry, hold exactly the FP64 pair set at the list radius
+    (the drop-in's cell_list_pairs, itself pinned to the reference's pair sets) on the positions of the last
+    rebuild, each pair in both directions; FP32c forces within the force tolerance of the FP64 plug-in's on
+    the same positions, energy within 2e-6, and the net force at round-off."""
+    from accusim import System
+
     from devinproj_b200 import GpuSimulation, cell_list_pairs, configs
-    from devinproj_b200.engine import forcefield_from
+    from tests.test_engine_lists_gpu import compare_sets, engine_pairs
     s, forces, dt = configs.lj_large(64)
     assert s.n == 1_048_576
     # the lattice's forces vanish by symmetry: displace every atom by a seeded 0.02 sigma first
     s.pos = (s.pos + np.random.default_rng(7).normal(0, 0.02 * configs.AR_SIGMA, s.pos.shape)) % s.box
-    _, rlist, _ = forcefield_from(forces, s.species)
+    sim = GpuSimulation(s, forces, dt=dt)
     for stage in ("initial", "after 200 steps"):
-        sim = GpuSimulation(s, forces, dt=dt)
-        i, j = cell_list_pairs(s, rlist)
-        assert sim.engine.neighbor_stats()[1] == 2 * len(i), stage
+        if stage != "initial":
+            sim.run(steps=200, record_every=100, positions=False)
+            assert sim.rebuilds >= 10
+        got, _, pos_build = engine_pairs(sim.engine)
+        b = System(3, box=s.box, periodic=True)
+        b.add_species("Ar", configs.AR_MASS)
+        b.add("Ar", pos_build)
+        i, j = cell_list_pairs(b, sim.rlist)
+        compare_sets(got, np.sort(i * s.n + j), pos_build, s.box, sim.rlist, f"1M LJ {stage}")
         F64 = np.zeros_like(s.pos)
         U64 = 0.0
         for f in forces:
@@ -290,10 +309,6 @@ def test_engine_full_size_lj1m_pair_set_forces_and_net_force():
         assert abs(sim.pe - U64) <= 2e-6 * abs(U64), stage
         frms = np.sqrt(np.mean(np.sum(F64 ** 2, 1)))
         assert np.linalg.norm(sim.force.sum(0)) <= 1e-6 * np.sqrt(s.n) * frms, stage
-        if stage == "initial":
-            sim.run(steps=200, record_every=100, positions=False)
-            assert sim.rebuilds >= 10
-        del sim
 
 
 def test_batched_replicas_equal_single_runs_bitwise():
@@ -349,7 +364,8 @@ def test_batched_nose_hoover_replicas_equal_single_runs_bitwise():
 
 
 def test_engine_rejects_unsupported_setups():
-    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones, System
+    from accusim import System
+    from devinproj_b200 import DampedShiftedCoulomb, GpuSimulation, LennardJones
     s = System(3, box=None)
     s.add_species("Ar", 6.6e-26)
     s.add("Ar", np.random.default_rng(0).uniform(0, 3e-9, (50, 3)))
@@ -390,13 +406,14 @@ def test_list_build_variants_agree(seed):
                         [("Ar", configs.AR_MASS, 0.0)])
         Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(st)
         assert rms_rel(out[tpa][3] * configs.AR_MASS, Fo) <= 1e-5
-    # fresh engines on identical positions: identical list totals and pair counts
+    # fresh engines on identical positions: identical pair sets (entry by entry) and pair counts
+    from tests.test_engine_lists_gpu import engine_pairs
     s.pos = out[1][2]
-    totals = []
+    sets = []
     for tpa in (1, 8):
         eng, _, _ = start_engine([s], [lj], [0.005 * configs.AR_TAU], tpa=tpa)
-        totals.append((eng.neighbor_stats()[1], eng.count_pairs()))
-    assert totals[0] == totals[1]
+        sets.append((engine_pairs(eng)[0], eng.count_pairs()))
+    assert np.array_equal(sets[0][0], sets[1][0]) and sets[0][1] == sets[1][1]
 
 
 @pytest.mark.parametrize("tpa", [1, 32])
@@ -410,11 +427,16 @@ def test_dense_cells_lists_match_oracle(tpa):
     s, forces, dt = configs.nacl4096(seed=3)
     s.pos = (s.pos + np.random.default_rng(7).normal(0, 0.2e-10, s.pos.shape)) % s.box
     s.vel[:] = 0.0
+    from tests._helpers import pair_keys
+    from tests.test_engine_lists_gpu import compare_sets, engine_pairs
     eng, rlist, _ = start_engine([s], forces, [dt], tpa=tpa)
     eng.check("start")
     st = oracle_of(s)
-    i, j = port.cell_list_pairs(st, rlist)
-    assert eng.neighbor_stats()[1] == 2 * len(i)
+    got, _, pos_build = engine_pairs(eng)
+    bst = port.State(pos_build, np.zeros_like(pos_build), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                     [(x.name, x.mass, x.charge) for x in s.species])
+    ref = pair_keys(*port.cell_list_pairs(bst, rlist), s.n)
+    assert compare_sets(got, ref, pos_build, s.box, rlist, f"dense cells tpa {tpa}") == 0
     p, v, a = eng.get_state()
     Fo = sum(f.compute(st)[0] for f in (port.LennardJones(configs.NACL_LJ, cutoff=2.5, skin=0.0),
                                          port.DampedShiftedCoulomb(rcut=forces[1].rcut, alpha=forces[1].alpha,
@@ -529,3 +551,35 @@ def test_list_overflow_mid_run_regrows_and_continues():
     assert len(sim.trajectory.t) == 5
     Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(oracle_of(s))
     assert rms_rel(sim.force, Fo) <= 1e-5
+
+
+def test_barrier_timeout_reports_and_returns():
+    """A bounded device wait that runs out (no fault, no hang): an engine whose grid-barrier waits give up at
+    once (barrier_wait_limit < 0) starts on a 32,000-atom fluid, so the first list build's cooperative kernel
+    (125 blocks; block 0 arrives last at the first barrier, after its prefix scan) has blocks that stop
+    waiting. The kernel returns, the status block carries ACS_FLAG_TIMEOUT, the host check raises
+    ACS_ERR_TIMEOUT (the reference raises its errors as Python exceptions, accusim/simulation.py:96-97), and
+    the engine's later kernels return at once. A new engine with the default limit then runs normally."""
+    import torch
+
+    from devinproj_b200 import _lib, configs
+    from devinproj_b200.engine import _upload_state, build_engine, start_engine
+    s, lj = configs.lj_fluid(20, seed=3)
+    dt = 0.005 * configs.AR_TAU
+    eng, _, _ = build_engine([dict(n=s.n, box=s.box, dt=dt)], [lj], s.species, barrier_wait_limit=-1)
+    assert eng.launch_info()[1] >= 100
+    _upload_state(eng, [s])            # set_state: the forced first rebuild
+    torch.cuda.synchronize()           # returned: no wait outlived its limit
+    assert eng.status().flags & _lib.FLAG_TIMEOUT
+    with pytest.raises(_lib.AcsError) as err:
+        eng.check("barrier timeout")
+    assert err.value.code == _lib.ACS_ERR_TIMEOUT
+    eng.run(5, 0, True)
+    torch.cuda.synchronize()
+    assert eng.status(clear=True).flags & _lib.FLAG_TIMEOUT
+    assert eng.status().flags == 0
+    del eng
+    ok, _, _ = start_engine([s], [lj], [dt])
+    ok.run(20, 10, True)
+    ok.check("default barrier limit")
+    assert np.all(np.isfinite(ok.records(2)))

@@ -1,0 +1,157 @@
+"""The engine's own neighbour lists (the ones behind the FP32c step) as pair sets, against the reference's pair
+search at the list radius (accusim/forces.py:279-321 cell_list_pairs, on the positions of the last rebuild,
+which the lists were built from; accusim/forces.py:86-98 VerletList.pairs rebuilds at rc + skin).
+
+Every list entry is decoded back to a pair of caller indices (acs_engine_dump_lists). Checked: no entry names
+a foreign or the same atom, every pair is listed in both directions exactly once, and the set of unordered pairs
+equals the reference's. A pair may differ only if it is an r^2 tie with the list radius (within 1e-12
+relative: the engine filters in Angstrom, the reference in metres); ties are counted and reported (none occur
+on these fixtures). DSF-excluded pairs stay listed with the exclusion flag set, exactly on the excluded pairs."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import accusim_port as port
+from tests._helpers import pair_keys
+
+pytestmark = pytest.mark.gpu
+
+TIE = 1e-12
+
+
+def engine_pairs(eng, r=None):
+    """(unordered pair keys i*n+j with i<j, sorted; excluded keys; build positions SI) of the engine's lists,
+    after the structural checks (foreign entries, self pairs, both directions, duplicates)."""
+    from devinproj_b200.engine import LEN
+    keys, pos = eng.list_entries()
+    keys = keys.cpu().numpy()
+    n = int(eng.offsets[-1])
+    assert np.all(keys >= 0), "a list entry names no atom of its own replica"
+    ex = (keys & 1).astype(bool)
+    d = keys >> 1
+    i, j = d // n, d % n
+    assert not np.any(i == j), "self pair in a list"
+    fwd = np.sort(i[i < j] * n + j[i < j])
+    bwd = np.sort(j[i > j] * n + i[i > j])
+    assert len(fwd) == len(bwd) and np.array_equal(fwd, bwd), "a pair is not listed in both directions"
+    assert np.all(np.diff(fwd) > 0), "a pair is listed twice"
+    exk = np.unique(np.minimum(i[ex], j[ex]) * n + np.maximum(i[ex], j[ex]))
+    return fwd, exk, pos.cpu().numpy() * LEN
+
+
+def compare_sets(got, ref, pos, box, rl, label):
+    """Pairs in exactly one of the two sets must be r^2 ties with rl^2; returns the number of ties."""
+    diff = np.setxor1d(got, ref)
+    n = len(pos)
+    for key in diff:
+        a, b = divmod(int(key), n)
+        dd = pos[b] - pos[a]
+        dd -= box * np.round(dd / box)
+        r2 = float(dd @ dd)
+        assert abs(r2 - rl * rl) <= TIE * rl * rl, f"{label}: pair {a},{b} (r/rl = {np.sqrt(r2) / rl:.9f}) differs"
+    print(f"{label}: {len(got)} pairs, {len(diff)} r^2 ties with the list radius")
+    return len(diff)
+
+
+def _system(g, suffix=""):
+    from tests.test_dropin_gpu import product_system
+    return product_system(g, suffix)
+
+
+@pytest.mark.parametrize("tpa", [1, 32])
+def test_engine_lists_equal_reference_pairs_argon864(golden, tpa):
+    from devinproj_b200.engine import start_engine
+    from devinproj_b200 import LennardJones
+    g = golden("argon864")
+    s = _system(g)
+    lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
+    eng, rlist, _ = start_engine([s], [lj], [float(g["dt"])], tpa=tpa)
+    got, _, pos = engine_pairs(eng)
+    assert np.max(np.abs(pos - s.pos)) <= 1e-15 * s.box[0]   # built from the golden positions (in Angstrom)
+    ref = pair_keys(g["pair_i"], g["pair_j"], s.n)
+    assert compare_sets(got, ref, pos, s.box, rlist, f"argon864 tpa {tpa}") == 0
+
+
+@pytest.mark.parametrize("kind", ["periodic", "ortho"])
+def test_engine_lists_equal_reference_pairs_lj_mixture(golden, kind):
+    from devinproj_b200.engine import start_engine
+    from devinproj_b200 import LennardJones
+    g = golden(f"lj_mix_{kind}")
+    s = _system(g)
+    params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+    eng, rlist, _ = start_engine([s], [LennardJones(params, cutoff=2.5)], [1e-15])
+    got, _, pos = engine_pairs(eng)
+    ref = pair_keys(g["pair_i"], g["pair_j"], s.n)
+    assert compare_sets(got, ref, pos, s.box, rlist, f"lj_mix_{kind}") == 0
+
+
+def test_engine_lists_match_reference_digest_nacl4096(golden):
+    """The 4096-ion NaCl lists (one list at the DSF list radius 13.8 A = rc + skin, the larger of the two
+    forces') hash to the reference's own pair set at 13.8 A; restricted to 12.32 A (the LJ list radius) the
+    listed pairs hash to the reference's LJ pair set."""
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones
+    from devinproj_b200.engine import start_engine
+    g = golden("nacl4096")
+    s = _system(g)
+    params = {str(n): (float(e), float(sg)) for n, e, sg in zip(g["param_names"], g["param_eps"], g["param_sig"])}
+    forces = [LennardJones(params, cutoff=2.5), DampedShiftedCoulomb(rcut=float(g["rcut"]), alpha=float(g["alpha"]))]
+    for tpa in (1, 16):
+        eng, rlist, _ = start_engine([s], forces, [float(g["dt"])], tpa=tpa)
+        assert rlist == pytest.approx(13.8e-10, rel=1e-12)
+        got, exk, pos = engine_pairs(eng)
+        assert len(exk) == 0 and np.max(np.abs(pos - s.pos)) <= 1e-15 * s.box[0]
+        assert len(got) == int(g["pairs_dsf_count"])
+        assert hashlib.sha256(got.tobytes()).hexdigest() == str(g["pairs_dsf_sha"]), tpa
+        i, j = divmod(got, s.n)
+        dd = s.pos[j] - s.pos[i]
+        dd -= s.box * np.round(dd / s.box)
+        inner = got[np.einsum("ij,ij->i", dd, dd) < (12.32e-10) ** 2]
+        assert len(inner) == int(g["pairs_lj_count"])
+        assert hashlib.sha256(inner.tobytes()).hexdigest() == str(g["pairs_lj_sha"]), tpa
+
+
+def test_engine_lists_after_rebuilds_equal_fresh_pair_search():
+    """Lists rebuilt inside graph-captured runs (hot argon, ~1 rebuild per few steps): after each of several
+    blocks, the engine's pair set equals the oracle's cell_list_pairs (the reference's algorithm, pinned
+    bit-exact to it) on the positions of the last rebuild, at the list radius."""
+    from devinproj_b200 import configs
+    from devinproj_b200.engine import start_engine
+    s, forces, dt = configs.argon864(seed=3)
+    s.maxwell_boltzmann(300.0, np.random.default_rng(3))
+    for tpa in (1, 32):
+        eng, rlist, _ = start_engine([s.copy()], forces, [dt], tpa=tpa)
+        rb0 = eng.status().rebuilds
+        for block in range(4):
+            eng.run(37, 0, True)
+            eng.check("run")
+            got, _, pos = engine_pairs(eng)
+            st = port.State(pos, np.zeros_like(pos), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                            [("Ar", configs.AR_MASS, 0.0)])
+            ref = pair_keys(*port.cell_list_pairs(st, rlist), s.n)
+            assert compare_sets(got, ref, pos, s.box, rlist, f"hot argon tpa {tpa} block {block}") == 0
+        assert eng.status().rebuilds - rb0 >= 8
+
+
+def test_engine_lists_flag_exactly_the_dsf_exclusions():
+    """With DSF exclusions the listed pair set is unchanged (the LJ term still needs those pairs) and the
+    exclusion flag sits exactly on the excluded pairs that lie inside the list radius."""
+    from devinproj_b200 import DampedShiftedCoulomb, LennardJones, configs
+    from devinproj_b200.engine import start_engine
+    s, forces, dt = configs.nacl4096(seed=1)
+    rng = np.random.default_rng(4)
+    ex = set()
+    while len(ex) < 300:
+        a, b = (int(x) for x in rng.integers(0, s.n, 2))
+        if a != b:
+            ex.add((min(a, b), max(a, b)))
+    dsf = DampedShiftedCoulomb(rcut=forces[1].rcut, alpha=forces[1].alpha, exclude=sorted(ex))
+    eng, rlist, _ = start_engine([s], [forces[0], dsf], [dt])
+    got, exk, pos = engine_pairs(eng)
+    eng0, _, _ = start_engine([s], forces, [dt])
+    got0, exk0, _ = engine_pairs(eng0)
+    assert np.array_equal(got, got0) and len(exk0) == 0
+    n = s.n
+    want = np.array(sorted(a * n + b for a, b in ex))
+    assert np.array_equal(exk, np.intersect1d(want, got))
+    assert len(exk) > 0
