@@ -1,6 +1,6 @@
 """Launch-shape autotuner for the engine: threads per atom in the pair kernel (1..32, which also fixes the
-neighbour-list layout). The step kernel's grid stays one thread per slot (`grid_mult` 0); a grid of k blocks
-per SM that loops over the slots (`grid_mult` k) is accepted by the engine but not searched.
+neighbour-list layout) and the step kernel's grid: one thread per slot (`grid_mult` 0), or k blocks per SM that
+loop over the slots (`grid_mult` 4 or 8), which trades the last wave's tail for a loop.
 
 `tune()` builds the engine for each candidate on the caller's own replicas, times a short eager run with
 CUDA events around every kernel (`acs_engine_run_timed`), and keeps the fastest step + list-maintenance
@@ -75,7 +75,7 @@ def candidates(n_total, nb):
     tpas = [t for t in (1, 2, 4, 8, 16, 32) if t * 4 <= max(nb, 4)]
     if n_total > 2_000_000:
         tpas = [t for t in tpas if t <= 4]
-    grids = [0]
+    grids = [0, 4, 8]
     return [(t, g) for t in tpas for g in grids]
 
 

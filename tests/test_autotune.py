@@ -29,12 +29,14 @@ def test_signature_buckets_and_distinguishes_workloads():
 
 
 def test_candidates():
-    # threads per atom: at most a quarter of the neighbours each, powers of two up to 32, the one-thread-per-slot grid
-    assert autotune.candidates(1000, 200) == [(t, 0) for t in (1, 2, 4, 8, 16, 32)]
-    assert autotune.candidates(1000, 40) == [(t, 0) for t in (1, 2, 4, 8)]
-    assert autotune.candidates(1000, 1) == [(1, 0)]
+    # threads per atom: at most a quarter of the neighbours each, powers of two up to 32; step grids of one thread
+    # per slot or 4 or 8 looping blocks per SM
+    g = (0, 4, 8)
+    assert autotune.candidates(1000, 200) == [(t, k) for t in (1, 2, 4, 8, 16, 32) for k in g]
+    assert autotune.candidates(1000, 40) == [(t, k) for t in (1, 2, 4, 8) for k in g]
+    assert autotune.candidates(1000, 1) == [(1, k) for k in g]
     # above two million atoms only 1, 2 or 4 threads per atom
-    assert autotune.candidates(3_000_000, 200) == [(1, 0), (2, 0), (4, 0)]
+    assert autotune.candidates(3_000_000, 200) == [(t, k) for t in (1, 2, 4) for k in g]
 
 
 def test_cache_round_trip_and_cached_answer(tmp_path, monkeypatch):
