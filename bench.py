@@ -260,12 +260,18 @@ def main():
                     help="steps of the plain FP64 plug-ins (device-resident GpuSystem in accusim's Simulation.run) "
                          "timed for the speed-up denominator; 0 skips them")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cell-order", type=int, default=0, choices=[0, 1],
+                    help="slot order of the cells: 0 row-major, 1 Morton")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
-    ap.add_argument("--experiment", choices=["learned", "drift", "dropin", "correction_kernels"], default=None,
+    ap.add_argument("--experiment", choices=["learned", "drift", "dropin", "correction_kernels", "autotune"],
+                    default=None,
                     help="accuracy experiments (one JSON line each): the learned DSF->Ewald correction at full scale, "
                          "the 1e4-step energy drift of the 1M-atom run, the plain FP64 drop-in's throughput")
     ap.add_argument("--snapshots", type=int, default=2000)
+    ap.add_argument("--train-configs", default="20:2e-3",
+                    help="learned experiment: comma-separated epochs:learning-rate settings, chosen on a validation "
+                         "split when there are several")
     ap.add_argument("--profile", action="store_true",
                     help="engine only: warm-up graph steps then --steps eager launches (for ncu), no timing legs")
     args = ap.parse_args()
@@ -311,7 +317,7 @@ def main():
         shard = shard_replicas([x.n for x in systems], world)[rank]
         systems, dts = [systems[r] for r in shard], [dts[r] for r in shard]
     rec_cap = max(args.steps // args.record_every + 2, args.drift_steps // args.record_every + 2, 4)
-    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=rec_cap, tpa=args.tpa)
+    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=rec_cap, tpa=args.tpa, cell_order=args.cell_order)
     n = sum(x.n for x in systems)
     pairs_lj, pairs_dsf = eng.count_pairs()
     step_blocks, coop_blocks, slots = eng.launch_info()
@@ -604,9 +610,22 @@ def run_experiment(args):
         d = generate_dataset(args.snapshots, seed=0, n_sites=20, verbose=False)
         t_gen = time.perf_counter() - t0
         n_train = int(0.9 * args.snapshots)
-        lc = LearnedCorrection(seed=0)
+        # training settings chosen on a validation split (the last 10% of the training snapshots), the error
+        # reported on the held-out 10% that no choice has seen
+        configs_tried = [tuple(float(x) for x in c.split(":")) for c in args.train_configs.split(",")]
+        n_fit = int(0.9 * n_train) if len(configs_tried) > 1 else n_train
+        val_idx = np.arange(n_fit, n_train)
+        trials = []
+        best = None
         t0 = time.perf_counter()
-        hist = lc.train(d, np.arange(n_train), epochs=20, batch_tiles=64, lr=2e-3)
+        for epochs, lr in configs_tried:
+            cand = LearnedCorrection(seed=0)
+            hist_c = cand.train(d, np.arange(n_fit), epochs=int(epochs), batch_tiles=64, lr=lr)
+            v = cand.errors(d, val_idx)[1] if len(val_idx) else float("nan")
+            trials.append({"epochs": int(epochs), "lr": lr, "val_rms_rel_err": v, "train_loss_last": hist_c[-1]})
+            if best is None or v < best[0]:
+                best = (v, cand, hist_c)
+        lc, hist = best[1], best[2]
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
         e0, e1 = lc.errors(d, np.arange(n_train, args.snapshots))
@@ -647,7 +666,7 @@ def run_experiment(args):
             graph_corr[stride] = graph_ms(corr.engine)
         print(json.dumps({"experiment": "learned_dsf_correction", "ions": 8000, "snapshots": args.snapshots,
                           "train_snapshots": n_train, "dataset_s": t_gen, "train_s": t_train,
-                          "train_loss_first_last": [hist[0], hist[-1]],
+                          "train_loss_first_last": [hist[0], hist[-1]], "training_trials": trials,
                           "heldout_rms_rel_err_dsf": e0, "heldout_rms_rel_err_corrected": e1, "error_ratio": e0 / e1,
                           "pair_kernel_bound": bound,
                           "step_ms_plain": step_plain, "correction_ms": c_ms,
@@ -689,6 +708,38 @@ def run_experiment(args):
         print(json.dumps({"experiment": "energy_drift_lj1m", "steps": steps, "record_every": every,
                           "energy_drift_report_metric": drift, "linear_drift_per_step_rel": slope,
                           "ms_per_step": e0.elapsed_time(e1) / steps, "rebuilds": eng.status().rebuilds}), flush=True)
+    elif args.experiment == "autotune":
+        # the tuned launch shape against the size rule on the ensemble's replica sizes: per bucket, 8 replicas of
+        # one fcc size at dt*, every candidate (threads per atom x step grid) timed with per-kernel events
+        from devinproj_b200 import autotune, configs
+        from devinproj_b200.engine import default_tpa, estimate_maxnb, forcefield_from, start_engine
+        rows = []
+        for nc in (4, 5, 6, 8, 10, 13, 16, 20):
+            systems = []
+            for k in range(8):
+                sk, lj = configs.lj_fluid(nc, seed=k)
+                systems.append(sk)
+            dts = [0.005 * configs.AR_TAU] * len(systems)
+            _, rlist, _ = forcefield_from([lj], systems[0].species)
+            n_total = sum(x.n for x in systems)
+            vol = sum(float(np.prod(x.box)) for x in systems)
+            nb = n_total / vol * 4.0 / 3.0 * math.pi * rlist ** 3
+            times = {}
+            for tpa, gm in autotune.candidates(n_total, nb):
+                eng, _, _ = start_engine([x.copy() for x in systems], [lj], dts, tpa=tpa, grid_mult=gm)
+                eng.run(10, 0, True)
+                k_ms, r_ms, tot = eng.run_timed(max(args.steps, 50), 0)
+                eng.check("autotune experiment")
+                times[f"{tpa},{gm}"] = tot / max(args.steps, 50)
+                del eng
+            cells = sum(int(np.prod([max(1, int(bx // rlist)) for bx in x.box])) for x in systems)
+            rule = default_tpa(n_total, (estimate_maxnb(systems[0].n, systems[0].box, rlist) - 32) / 1.3, cells)
+            best = min(times, key=times.get)
+            rows.append({"atoms_per_replica": systems[0].n, "replicas": len(systems), "rule": f"{rule},0",
+                         "rule_ms": times.get(f"{rule},0"), "best": best, "best_ms": times[best],
+                         "gain": (times.get(f"{rule},0") or float("nan")) / times[best], "ms_per_step": times})
+            print(json.dumps(rows[-1]), flush=True)
+        print(json.dumps({"experiment": "autotune_vs_size_rule", "rows": len(rows)}), flush=True)
     elif args.experiment == "dropin":
         # the FP64 plug-ins inside accusim's Simulation.run: on a device-resident GpuSystem (the honest FP64 GPU
         # figure) and on accusim's plain System (state copied to and from the host every step)

@@ -22,6 +22,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <vector>
 
@@ -41,6 +42,7 @@ constexpr int kCellChunk = 1024;  // cell-scan chunk (4 cells per thread of a 25
 constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
+constexpr int kListStage = 16;   // list rows staged per home atom in the warp-per-cell list build
 constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
 
 struct RepDev {
@@ -98,6 +100,10 @@ struct Eng {
   double *xa, *tmp_xa, *tmp_v;
   int32_t *tmp_cell, *tmp_id, *tmp_sp, *newcell, *perm, *perm2;
   int32_t *count, *start, *cursor;
+  // slot order of cells: cells' atoms occupy consecutive slots in the order given by crank (cell id -> position,
+  // both global over replicas); start[] is indexed by position, so the atoms of cell c are the slots
+  // [start[crank[c]], start[crank[c] + 1]). cell_at is the inverse (position -> cell id).
+  int32_t *crank, *cell_at;
   double *partials, *chunk_part, *rec;
   int32_t rec_cap;
   acs_dev_status* status;
@@ -958,7 +964,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int idx = 4 * threadIdx.x + q;
-      v[q] = idx < nc ? E.count[c0 + idx] : 0;
+      v[q] = idx < nc ? E.count[E.cell_at[c0 + idx]] : 0;
       sum += v[q];
     }
     int total;
@@ -1000,7 +1006,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     const int r = E.tile_rep[s >> 5];
     if (!fl[r] || s - E.rep[r].atom0 >= E.rep[r].n) continue;
     const int c = E.newcell[s];
-    E.perm[E.start[c] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
+    E.perm[E.start[E.crank[c]] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
   }
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(7);
@@ -1010,7 +1016,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
     const int v = E.perm[k];
     const int c = E.newcell[v];
-    const int a0 = E.start[c], a1 = E.start[c + 1];
+    const int a0 = E.start[E.crank[c]], a1 = E.start[E.crank[c] + 1];
     int rank = 0;
     for (int a = a0; a < a1; ++a) rank += (E.perm[a] < v);
     E.perm2[a0 + rank] = v;
@@ -1083,7 +1089,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
           for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
             const int cc = ps.cell(a, b, d);
-            const int k0 = E.start[cc], k1 = E.start[cc + 1];
+            const int k0 = E.start[E.crank[cc]], k1 = E.start[E.crank[cc] + 1];
             for (int base = k0; base < k1; base += 32) {
               const int k = base + lane;
               int code = -1;
@@ -1114,6 +1120,13 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     __shared__ float4 bufp[8][64];
     __shared__ uint32_t bufk[8][64];
     __shared__ int selfpos[8][32];
+    // Staged list stores: lane h keeps its home atom's last kListStage entries in its own column of this ring
+    // (conflict-free: one bank per lane) until every home atom of the chunk has produced that list position;
+    // such a row is then written with one store per lane, all lanes at the same position, so the lanes of a
+    // 32-slot group write one contiguous run instead of one sector each. An entry that would overrun the ring
+    // (its atom is kListStage positions ahead of the slowest one) and every later entry of that atom go to
+    // global memory directly.
+    __shared__ uint32_t ring[8][kListStage][32];
     const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -1130,7 +1143,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         }
       }
       const RepDev& R = E.rep[r];
-      const int64_t c = R.cellbase + (f - __ldcg(E.fcell + r));
+      const int64_t c = E.cell_at[R.cellbase + (f - __ldcg(E.fcell + r))];   // home cells in slot order
       const float4* __restrict__ im = E.img[dst];
       const float rl2f = (float)R.rl2, lo_f = rl2f * (1.0f - 1e-4f), hi_f = rl2f * (1.0f + 1e-4f);
       // stencil cell st = 9 (a + 1) + 3 (b + 1) + (d + 1) in list order: lane st holds its first slot, its
@@ -1142,8 +1155,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         const int n0 = wrapc(c0 + lane / 9 - 1, R.nc[0]), n1 = wrapc(c1 + (lane / 3) % 3 - 1, R.nc[1]),
                   n2 = wrapc(c2 + lane % 3 - 1, R.nc[2]);
         const int cc = R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + n2;
-        sk0 = E.start[cc];
-        slen = E.start[cc + 1] - sk0;
+        sk0 = E.start[E.crank[cc]];
+        slen = E.start[E.crank[cc] + 1] - sk0;
       }
       int incl = slen;
 #pragma unroll
@@ -1190,6 +1203,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         hpos[wib][lane] = im[i];
         int32_t* __restrict__ lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
         int cnt = 0, nbuf = 0, rb = 0;
+        int direct_from = INT_MAX;   // this lane's first list position written past the ring
+        int flushed = 0;             // rows [0, flushed) of every home atom are in global memory (warp-uniform)
         float4 rp;
         uint32_t rk;
         bool rkeep;
@@ -1253,10 +1268,20 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
             if (cnt < E.maxnb) {
               uint32_t v = bufk[wib][t];
               if (EX && dsf_excluded(E, E.id[i], E.id[v & kIdxMask])) v |= E.ex_bit;
-              lst[(int64_t)cnt * E.G] = (int32_t)v;
+              if (cnt < direct_from && cnt - flushed < kListStage) {
+                ring[wib][cnt % kListStage][lane] = v;
+              } else {
+                direct_from = min(direct_from, cnt);
+                lst[(int64_t)cnt * E.G] = (int32_t)v;
+              }
             }
             ++cnt;
           }
+          // rows every home atom has reached: one coalesced store per row
+          const int done_rows = __reduce_min_sync(0xffffffffu, own ? min(cnt, E.maxnb) : INT_MAX);
+          for (int p = flushed; p < done_rows; ++p)
+            if (own && p < direct_from) lst[(int64_t)p * E.G] = (int32_t)ring[wib][p % kListStage][lane];
+          flushed = max(flushed, done_rows);
           // keep the survivors beyond this batch at the front of the buffer
           __syncwarp();
           const int rest = nbuf - nk;
@@ -1273,6 +1298,15 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           }
           nbuf = rest;
         }
+        // the rows left in the ring once the candidates are exhausted
+        const int last_row = __reduce_max_sync(0xffffffffu, own ? min(cnt, E.maxnb) : 0);
+        for (int p = flushed; p < last_row; ++p)
+          if (own && p < min(cnt, E.maxnb) && p < direct_from)
+            lst[(int64_t)p * E.G] = (int32_t)ring[wib][p % kListStage][lane];
+        // count of entries that bypassed the ring (diagnostic, read with the phase times)
+        const int unstaged = __reduce_add_sync(0xffffffffu, own && direct_from < min(cnt, E.maxnb)
+                                                                ? min(cnt, E.maxnb) - direct_from : 0);
+        if (lane == 0 && unstaged) atomicAdd(&E.phase_ns[13], (unsigned long long)unstaged);
         if (own) {
           E.nnb[i] = min(cnt, E.maxnb);
           if (cnt > E.maxnb) {
@@ -1295,7 +1329,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
             if (ps.cell_beyond(a, b, d)) continue;
             const int cc = ps.cell(a, b, d);
-            const int k0 = E.start[cc], k1 = E.start[cc + 1];
+            const int k0 = E.start[E.crank[cc]], k1 = E.start[E.crank[cc] + 1];
             for (int k = k0; k < k1; k += 4) {
               float q[4];
               ps.screen4(k, k1, a, b, d, q);
@@ -1606,6 +1640,17 @@ struct Layout {
   }
 };
 
+// Interleave the low 10 bits of three coordinates (z fastest): the Morton (Z-order) key of a cell.
+uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+uint32_t morton3(uint32_t a, uint32_t b, uint32_t c) { return (spread10(a) << 2) | (spread10(b) << 1) | spread10(c); }
+
 int tpa_of(const acs_engine_config* cfg) {
   const int t = cfg->tpa;
   return (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32) ? t : (t == 0 ? 1 : -1);
@@ -1620,6 +1665,10 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
   }
   const int G = 32 / tpa;
   err = ACS_OK;
+  if (cfg->cell_order != 0 && cfg->cell_order != 1) {
+    err = ACS_ERR_ARG;
+    return;
+  }
   if (cfg->thermo.kind < 0 || cfg->thermo.kind > 2 ||
       (cfg->thermo.kind == 1 && !(cfg->thermo.kT >= 0.0 && cfg->thermo.friction >= 0.0)) ||
       (cfg->thermo.kind == 2 && !(cfg->thermo.kT > 0.0 && cfg->thermo.period > 0.0))) {
@@ -1772,6 +1821,8 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(4 * ((size_t)R + 1));                // 47 flagged-cell prefix of a rebuild
   L.add(4 * ((size_t)n_ex_ids + 1));         // 48 DSF exclusions: CSR starts by atom id
   L.add(4 * ((size_t)n_ex + 1));             // 49 DSF exclusions: excluded ids
+  L.add(4 * (size_t)C);                      // 50 crank (cell id -> slot-order position)
+  L.add(4 * (size_t)C);                      // 51 cell_at (position -> cell id)
   return L;
 }
 
@@ -2052,6 +2103,8 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.n_ex_ids = cfg->n_ex_ids;
   E.ex_start = (const int32_t*)(b + L.off[48]);
   E.ex_ids = (const int32_t*)(b + L.off[49]);
+  E.crank = (int32_t*)(b + L.off[50]);
+  E.cell_at = (int32_t*)(b + L.off[51]);
   E.ex_bit = cfg->n_ex_ids > 0 ? kExBit : 0u;
   E.jmask = cfg->n_ex_ids > 0 ? kExBit - 1u : kIdxMask;
   E.thermo = cfg->thermo.kind;
@@ -2062,8 +2115,26 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   // host-built index tables
   std::vector<int32_t> tile_rep(T), cell_rep(C), chunk_rep(NCH), chunk_t0(NCH), chunk_nt(NCH);
   std::vector<int32_t> cc_rep(NCC), cc_c0(NCC), cc_n(NCC);
+  std::vector<int32_t> crank(C), cell_at(C);
   for (int r = 0; r < E.R; ++r) {
     const RepDev& R = e->reps[r];
+    // slot order of the replica's cells: row-major (cell_order 0), or Morton (Z) order of the cell coordinates
+    // (cell_order 1), which keeps the cells of one block of slots, and so their 27-cell neighbourhoods, compact
+    std::vector<int32_t> order(R.ncells);
+    for (int c = 0; c < R.ncells; ++c) order[c] = c;
+    if (cfg->cell_order == 1) {
+      std::vector<uint32_t> key(R.ncells);
+      for (int c = 0; c < R.ncells; ++c) {
+        const int c2 = c % R.nc[2], c1 = (c / R.nc[2]) % R.nc[1], c0 = c / (R.nc[2] * R.nc[1]);
+        key[c] = morton3((uint32_t)c0, (uint32_t)c1, (uint32_t)c2);
+      }
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return key[a] < key[b2]; });
+    }
+    for (int p = 0; p < R.ncells; ++p) {
+      cell_at[R.cellbase + p] = R.cellbase + order[p];
+      crank[R.cellbase + order[p]] = R.cellbase + p;
+    }
+    crank[R.cellbase + R.ncells] = cell_at[R.cellbase + R.ncells] = R.cellbase + R.ncells;   // sentinel
     for (int t = 0; t < R.ntiles; ++t) tile_rep[R.tile0 + t] = r;
     for (int c = 0; c <= R.ncells; ++c) cell_rep[R.cellbase + c] = r;
     for (int c = 0; c < R.ncc; ++c) {
@@ -2101,6 +2172,8 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   }
   ok = ok && cudaMemcpy(E.bar, bar0, 16, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(e->src0_dev, e->src0.data(), 8 * (size_t)E.R, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.crank, crank.data(), 4 * (size_t)C, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(E.cell_at, cell_at.data(), 4 * (size_t)C, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.cc_rep, cc_rep.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.cc_c0, cc_c0.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(E.cc_n, cc_n.data(), 4 * (size_t)NCC, cudaMemcpyHostToDevice) == cudaSuccess;

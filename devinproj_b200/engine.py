@@ -54,7 +54,7 @@ class Thermostat(C.Structure):
 
 class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
-                ("tpa", C.c_int32), ("pad", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
+                ("tpa", C.c_int32), ("cell_order", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
                 ("thermo", Thermostat), ("ex_start", C.POINTER(C.c_int32)), ("ex_ids", C.POINTER(C.c_int32)),
                 ("n_ex_ids", C.c_int32), ("pad2", C.c_int32), ("barrier_wait_limit", C.c_int64)]
 
@@ -158,7 +158,7 @@ class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
     def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
-                 thermo=None, exclusions=None, barrier_wait_limit: int = 0):
+                 thermo=None, exclusions=None, barrier_wait_limit: int = 0, cell_order: int = 0):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -178,6 +178,8 @@ class Engine:
         self.cfg = EngineConfig(self.R, int(maxnb), int(rec_cap), int(grid_mult), self.tpa, 0, self._reps, ff,
                                 thermo if thermo is not None else Thermostat())
         self.cfg.barrier_wait_limit = int(barrier_wait_limit)
+        self.cfg.cell_order = int(cell_order)
+        self.cell_order = int(cell_order)
         self._ex = exclusions   # (ex_start, ex_ids) int32 arrays, kept alive with the config
         if exclusions is not None:
             ex_start, ex_ids = exclusions
@@ -299,10 +301,13 @@ class Engine:
               9: "gather", 10: "commit", 15: "list_build_block0"}
 
     def phase_times(self, clear=True):
-        """List-maintenance phase times (ms, accumulated) from the device global timer."""
+        """List-maintenance phase times (ms, accumulated) from the device global timer, and the number of list
+        entries the warp-per-cell build wrote past its staging ring ("list_entries_unstaged")."""
         out = np.zeros(16, dtype=np.uint64)
         _lib.check(self.L.acs_engine_phase_times(self.h, out.ctypes.data, 1 if clear else 0), "phase_times")
-        return {name: float(out[k]) / 1e6 for k, name in self.PHASES.items()}
+        res = {name: float(out[k]) / 1e6 for k, name in self.PHASES.items()}
+        res["list_entries_unstaged"] = int(out[13])
+        return res
 
     def records(self, count: int) -> np.ndarray:
         """(count, R, 8) FP64 records [KE, PE, Px, Py, Pz, Lx, Ly, Lz] in engine units."""
@@ -402,7 +407,7 @@ def dsf_exclusions(forces, systems):
 
 
 def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None,
-                 exclusions=None, barrier_wait_limit=0):
+                 exclusions=None, barrier_wait_limit=0, cell_order=0):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -415,7 +420,8 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
         cells = sum(int(np.prod([max(1, int(bx // r["rlist"])) for bx in r["box"]])) for r in reps)
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3, cells)
     return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
-                   exclusions=exclusions, barrier_wait_limit=barrier_wait_limit), rlist, half_skin)
+                   exclusions=exclusions, barrier_wait_limit=barrier_wait_limit, cell_order=cell_order), rlist,
+            half_skin)
 
 
 def _upload_state(engine, systems):
@@ -431,7 +437,7 @@ def _upload_state(engine, systems):
     engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
 
 
-def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None):
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None, cell_order=0):
     """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
     grows the neighbour capacity once if the first build overflows."""
     for s in systems:
@@ -445,7 +451,7 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=
     ex = dsf_exclusions(forces, systems)
     for attempt in range(3):
         eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,
-                                      tpa=tpa, thermo=thermo, exclusions=ex)
+                                      tpa=tpa, thermo=thermo, exclusions=ex, cell_order=cell_order)
         _upload_state(eng, systems)
         st = eng.status()
         if st.flags & _lib.FLAG_OVERFLOW:

@@ -1,7 +1,8 @@
 """Generate the golden vectors the parity tests pin against, by running the reference accusim itself.
 
-Run where the reference checkout is importable (it is read from $ACCUSIM_REF, default
-/root/reference):  python tests/golden/make_golden.py
+Run where the reference is importable: from $ACCUSIM_REF (a checkout of the reference project), else from the
+repository's offline install under baseline/_ref (baseline/install_reference.sh), else an installed accusim:
+    ACCUSIM_REF=<checkout> python tests/golden/make_golden.py
 The .npz files it writes are committed; nothing at test time imports the reference.
 
 Each case restates a reference test or example setup (file:line inside the accusim project):
@@ -34,8 +35,11 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("ACCUSIM_REF", "/root/reference")
-sys.path.insert(0, REF)
+_INSTALL = os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "baseline",
+                        "_ref")
+REF = os.environ.get("ACCUSIM_REF") or (_INSTALL if os.path.isdir(os.path.join(_INSTALL, "accusim")) else None)
+if REF:
+    sys.path.insert(0, REF)
 import accusim  # noqa: E402
 from accusim import Q, Simulation, System, VelocityVerlet, k_B  # noqa: E402
 from accusim.integrators import Langevin, NoseHoover  # noqa: E402
