@@ -687,10 +687,19 @@ def run_experiment(args):
                           "step_kernel_ms": step_ms, "list_kernel_ms": list_ms,
                           "correction_ms": sim.engine.last_correction_ms()}), flush=True)
     elif args.experiment == "drift":
+        # the report's energy-drift metric over 10^4 steps of the 1M-atom fluid from its initial state: the FP32c
+        # engine, and the plain FP64 plug-ins inside accusim's Simulation.run on a device-resident GpuSystem from
+        # the same state (the reference model's own drift at this dt, with no FP32 arithmetic)
+        from devinproj_b200 import VelocityVerlet
+        from devinproj_b200._accusim import simulation as _asim
         from devinproj_b200.engine import start_engine
+        from devinproj_b200.ensemble import drift_of
+        from devinproj_b200.state import GpuSystem
+        steps, every = args.drift_steps or 10000, 100
         s, forces, dt, cfg = workload("lj1m", seed=0)
-        eng, _, _ = start_engine([s], forces, [dt], rec_cap=128)
-        steps, every = 10000, 100
+        s64 = GpuSystem.from_system(s)
+        eng, _, _ = start_engine([s], forces, [dt], rec_cap=steps // every + 2)
+        init = eng.records(1)[0, 0].copy()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -698,16 +707,33 @@ def run_experiment(args):
         e1.record()
         torch.cuda.synchronize()
         eng.check("drift run")
-        rec = eng.records(steps // every)[:, 0, :]
-        init = None
+        rec = np.concatenate([init[None], eng.records(steps // every)[:, 0, :]])
+        drift32 = drift_of(rec[:, 0], rec[:, 1])
         E = rec[:, 0] + rec[:, 1]
         scale = max(abs(E[0]), np.max(np.abs(rec[:, 0])), np.max(np.abs(rec[:, 1])))
-        drift = float(np.max(np.abs(E - E[0])) / scale)
-        slope = float(np.polyfit(np.arange(len(E)) * every, E, 1)[0]) / scale
-        del init
-        print(json.dumps({"experiment": "energy_drift_lj1m", "steps": steps, "record_every": every,
-                          "energy_drift_report_metric": drift, "linear_drift_per_step_rel": slope,
-                          "ms_per_step": e0.elapsed_time(e1) / steps, "rebuilds": eng.status().rebuilds}), flush=True)
+        slope32 = float(np.polyfit(np.arange(len(E)) * every, E, 1)[0]) / scale
+        ms32 = e0.elapsed_time(e1) / steps
+        rebuilds32 = eng.status().rebuilds
+        del eng
+        out = {"experiment": "energy_drift_lj1m", "steps": steps, "record_every": every, "records": len(E),
+               "fp32c": {"energy_drift_report_metric": drift32, "linear_drift_per_step_rel": slope32,
+                         "ms_per_step": ms32, "rebuilds": rebuilds32}}
+        if args.fp64_steps > 0:
+            sim = _asim.Simulation(s64, forces, integrator=VelocityVerlet(), dt=dt)
+            t0 = time.perf_counter()
+            tr = sim.run(steps=steps, record_every=every, positions=False)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            KE, PE = np.array(tr.kinetic), np.array(tr.potential)
+            E64 = KE + PE
+            sc64 = max(abs(E64[0]), np.max(np.abs(KE)), np.max(np.abs(PE)))
+            out["fp64_dropin"] = {"energy_drift_report_metric": drift_of(KE, PE),
+                                  "linear_drift_per_step_rel": float(np.polyfit(np.arange(len(E64)) * every, E64, 1)[0])
+                                  / sc64, "wall_s": wall, "records": len(E64),
+                                  "path": "accusim.Simulation.run + GpuSystem + FP64 plug-ins"}
+            n = min(len(E64), len(E))
+            out["max_energy_difference_fp32c_vs_fp64_rel"] = float(np.max(np.abs(E[:n] - E64[:n])) / sc64)
+        print(json.dumps(out), flush=True)
     elif args.experiment == "autotune":
         # the tuned launch shape against the size rule on the ensemble's replica sizes: per bucket, 8 replicas of
         # one fcc size at dt*, every candidate (threads per atom x step grid) timed with per-kernel events

@@ -238,7 +238,7 @@ def test_nacl4096_lj_plus_dsf_matches_reference(golden):
     tr = sim.run(steps=int(g["steps"]), positions=False)
     assert rel_max(np.array(tr.kinetic), g["kinetic"]) <= 1e-11
     assert rel_max(np.array(tr.potential), g["potential"]) <= 1e-11
-    assert lj.rebuilds == int(g["rebuilds_lj"]) and dsf.rebuilds == int(g["rebuilds_dsf"])
+    assert lj.rebuilds == int(g["rebuilds_lj"]) and dsf._vl.rebuilds == int(g["rebuilds_dsf"])
 
 
 def test_forces_are_negative_gradient_and_newton3():
