@@ -23,6 +23,17 @@ __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, 
 // d -= box * np.round(d / box)   (np.round: half to even == rint)
 __device__ __forceinline__ double min_image(double d, double box) { return sub(d, mul(box, rint(div(d, box)))); }
 
+// The same, bit for bit, with a multiply by 1/box in place of the division for almost every pair: t = d (1/box)
+// differs from the IEEE quotient d / box by under 3e-16 |d / box|, and rint only changes at half-integers, so
+// rint(t) is rint(d / box) unless t lies within 1e-9 of a half-integer (or |t| is huge); there the quotient
+// decides as in the reference.
+__device__ __forceinline__ double min_image(double d, double box, double inv_box) {
+  const double t = d * inv_box;
+  const double f = fabs(t - trunc(t));
+  const double k = (fabs(f - 0.5) > 1e-9 && fabs(t) < 1e6) ? rint(t) : rint(div(d, box));
+  return sub(d, mul(box, k));
+}
+
 // np.einsum("ij,ij->i") over 3 components, summed left to right without FMA.
 __device__ __forceinline__ double norm2(double dx, double dy, double dz) {
   return add(add(mul(dx, dx), mul(dy, dy)), mul(dz, dz));
@@ -30,14 +41,15 @@ __device__ __forceinline__ double norm2(double dx, double dy, double dz) {
 
 struct Box3 {
   double L[3];
+  double inv[3];   // 1 / L, for min_image's multiply
   int periodic;
 };
 
 __device__ __forceinline__ void min_image3(double& dx, double& dy, double& dz, const Box3& b) {
   if (b.periodic) {
-    dx = min_image(dx, b.L[0]);
-    dy = min_image(dy, b.L[1]);
-    dz = min_image(dz, b.L[2]);
+    dx = min_image(dx, b.L[0], b.inv[0]);
+    dy = min_image(dy, b.L[1], b.inv[1]);
+    dz = min_image(dz, b.L[2], b.inv[2]);
   }
 }
 

@@ -28,6 +28,7 @@ GridDev to_dev(const acs_grid* g) {
     d.lo[k] = g->lo[k];
     d.span[k] = g->span[k];
     d.box.L[k] = g->box[k];
+    d.box.inv[k] = g->box[k] != 0.0 ? 1.0 / g->box[k] : 0.0;
     d.nc[k] = g->ncell[k];
   }
   d.box.periodic = g->periodic;
@@ -318,10 +319,11 @@ __global__ void __launch_bounds__(kBlock) k_lj64(const double* __restrict__ pos,
       const int p = si + sp[j];
       const double e = t.eps[p];
       if (r2 < t.rc2[p] && e > 0.0) {
-        const double sr2 = t.sig2[p] / r2;
+        const double ir2 = 1.0 / r2;
+        const double sr2 = t.sig2[p] * ir2;
         const double sr6 = sr2 * sr2 * sr2;
         u += 4.0 * e * (sr6 * sr6 - sr6 - t.shift6);
-        const double coef = -24.0 * e * (2.0 * sr6 * sr6 - sr6) / r2;
+        const double coef = -24.0 * e * (2.0 * sr6 * sr6 - sr6) * ir2;
         fx += coef * dx;
         fy += coef * dy;
         fz += coef * dz;
@@ -362,8 +364,9 @@ __global__ void __launch_bounds__(kBlock) k_dsf64(const double* __restrict__ pos
       const double qq = qi * q[j];
       const double ar = P.a * r;
       const double er = erfc(ar);
-      u += qq * (er / r - P.erc / P.rc + P.fshift * (r - P.rc));
-      const double fv = qq * ((er / (r * r) + P.c * exp(-(ar * ar)) / r) - P.fshift) / r;
+      const double ir = 1.0 / r;
+      u += qq * (er * ir - P.erc / P.rc + P.fshift * (r - P.rc));
+      const double fv = qq * ((er * (ir * ir) + P.c * exp(-(ar * ar)) * ir) - P.fshift) * ir;
       fx -= fv * dx;
       fy -= fv * dy;
       fz -= fv * dz;
@@ -448,7 +451,10 @@ __global__ void __launch_bounds__(kBlock) k_conserved(const double* __restrict__
 
 inline Box3 make_box(const double* box3, int periodic) {
   Box3 b;
-  for (int k = 0; k < 3; ++k) b.L[k] = box3 ? box3[k] : 0.0;
+  for (int k = 0; k < 3; ++k) {
+    b.L[k] = box3 ? box3[k] : 0.0;
+    b.inv[k] = b.L[k] != 0.0 ? 1.0 / b.L[k] : 0.0;
+  }
   b.periodic = (periodic && box3) ? 1 : 0;
   return b;
 }
