@@ -260,8 +260,8 @@ def main():
                     help="steps of the plain FP64 plug-ins (device-resident GpuSystem in accusim's Simulation.run) "
                          "timed for the speed-up denominator; 0 skips them")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cell-order", type=int, default=0, choices=[0, 1],
-                    help="slot order of the cells: 0 row-major, 1 Morton")
+    ap.add_argument("--cell-order", type=int, default=1, choices=[0, 1],
+                    help="slot order of the cells: 1 Morton (default), 0 row-major")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
     ap.add_argument("--experiment", choices=["learned", "drift", "dropin", "correction_kernels", "autotune"],

@@ -22,7 +22,6 @@
 #include <math.h>
 
 #include <algorithm>
-#include <climits>
 #include <map>
 #include <vector>
 
@@ -42,7 +41,6 @@ constexpr int kCellChunk = 1024;  // cell-scan chunk (4 cells per thread of a 25
 constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
-constexpr int kListStage = 16;   // list rows staged per home atom in the warp-per-cell list build
 constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
 
 struct RepDev {
@@ -1120,13 +1118,6 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     __shared__ float4 bufp[8][64];
     __shared__ uint32_t bufk[8][64];
     __shared__ int selfpos[8][32];
-    // Staged list stores: lane h keeps its home atom's last kListStage entries in its own column of this ring
-    // (conflict-free: one bank per lane) until every home atom of the chunk has produced that list position;
-    // such a row is then written with one store per lane, all lanes at the same position, so the lanes of a
-    // 32-slot group write one contiguous run instead of one sector each. An entry that would overrun the ring
-    // (its atom is kListStage positions ahead of the slowest one) and every later entry of that atom go to
-    // global memory directly.
-    __shared__ uint32_t ring[8][kListStage][32];
     const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -1203,8 +1194,6 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         hpos[wib][lane] = im[i];
         int32_t* __restrict__ lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
         int cnt = 0, nbuf = 0, rb = 0;
-        int direct_from = INT_MAX;   // this lane's first list position written past the ring
-        int flushed = 0;             // rows [0, flushed) of every home atom are in global memory (warp-uniform)
         float4 rp;
         uint32_t rk;
         bool rkeep;
@@ -1268,20 +1257,10 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
             if (cnt < E.maxnb) {
               uint32_t v = bufk[wib][t];
               if (EX && dsf_excluded(E, E.id[i], E.id[v & kIdxMask])) v |= E.ex_bit;
-              if (cnt < direct_from && cnt - flushed < kListStage) {
-                ring[wib][cnt % kListStage][lane] = v;
-              } else {
-                direct_from = min(direct_from, cnt);
-                lst[(int64_t)cnt * E.G] = (int32_t)v;
-              }
+              lst[(int64_t)cnt * E.G] = (int32_t)v;
             }
             ++cnt;
           }
-          // rows every home atom has reached: one coalesced store per row
-          const int done_rows = __reduce_min_sync(0xffffffffu, own ? min(cnt, E.maxnb) : INT_MAX);
-          for (int p = flushed; p < done_rows; ++p)
-            if (own && p < direct_from) lst[(int64_t)p * E.G] = (int32_t)ring[wib][p % kListStage][lane];
-          flushed = max(flushed, done_rows);
           // keep the survivors beyond this batch at the front of the buffer
           __syncwarp();
           const int rest = nbuf - nk;
@@ -1298,15 +1277,6 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           }
           nbuf = rest;
         }
-        // the rows left in the ring once the candidates are exhausted
-        const int last_row = __reduce_max_sync(0xffffffffu, own ? min(cnt, E.maxnb) : 0);
-        for (int p = flushed; p < last_row; ++p)
-          if (own && p < min(cnt, E.maxnb) && p < direct_from)
-            lst[(int64_t)p * E.G] = (int32_t)ring[wib][p % kListStage][lane];
-        // count of entries that bypassed the ring (diagnostic, read with the phase times)
-        const int unstaged = __reduce_add_sync(0xffffffffu, own && direct_from < min(cnt, E.maxnb)
-                                                                ? min(cnt, E.maxnb) - direct_from : 0);
-        if (lane == 0 && unstaged) atomicAdd(&E.phase_ns[13], (unsigned long long)unstaged);
         if (own) {
           E.nnb[i] = min(cnt, E.maxnb);
           if (cnt > E.maxnb) {

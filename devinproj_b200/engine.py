@@ -158,7 +158,7 @@ class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
     def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
-                 thermo=None, exclusions=None, barrier_wait_limit: int = 0, cell_order: int = 0):
+                 thermo=None, exclusions=None, barrier_wait_limit: int = 0, cell_order: int = 1):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -301,13 +301,10 @@ class Engine:
               9: "gather", 10: "commit", 15: "list_build_block0"}
 
     def phase_times(self, clear=True):
-        """List-maintenance phase times (ms, accumulated) from the device global timer, and the number of list
-        entries the warp-per-cell build wrote past its staging ring ("list_entries_unstaged")."""
+        """List-maintenance phase times (ms, accumulated) from the device global timer."""
         out = np.zeros(16, dtype=np.uint64)
         _lib.check(self.L.acs_engine_phase_times(self.h, out.ctypes.data, 1 if clear else 0), "phase_times")
-        res = {name: float(out[k]) / 1e6 for k, name in self.PHASES.items()}
-        res["list_entries_unstaged"] = int(out[13])
-        return res
+        return {name: float(out[k]) / 1e6 for k, name in self.PHASES.items()}
 
     def records(self, count: int) -> np.ndarray:
         """(count, R, 8) FP64 records [KE, PE, Px, Py, Pz, Lx, Ly, Lz] in engine units."""
@@ -407,7 +404,7 @@ def dsf_exclusions(forces, systems):
 
 
 def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None,
-                 exclusions=None, barrier_wait_limit=0, cell_order=0):
+                 exclusions=None, barrier_wait_limit=0, cell_order=1):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -437,7 +434,7 @@ def _upload_state(engine, systems):
     engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
 
 
-def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None, cell_order=0):
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None, cell_order=1):
     """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
     grows the neighbour capacity once if the first build overflows."""
     for s in systems:

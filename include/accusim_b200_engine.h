@@ -125,8 +125,7 @@ int acs_engine_launch_info(acs_engine* e, int32_t* step_blocks, int32_t* coop_bl
 int acs_engine_run_timed(acs_engine* e, int32_t steps, int32_t record_every, float* out_ms, void* stream);
 /* Accumulated wall time (ns, device global timer, block 0's view) of the list-maintenance phases:
  * [1] flag read, [2] clear, [3] bin, [4..6] scan, [7] scatter, [8] in-cell sort, [9] gather, [10] commit,
- * [15] list build (block 0 share); [13] is a count, not a time: list entries the warp-per-cell build wrote
- * directly instead of through its staging ring. Synchronous. */
+ * [15] list build (block 0 share). Synchronous. */
 int acs_engine_phase_times(acs_engine* e, unsigned long long* out16, int clear);
 /* Learned force correction (no counterpart in the reference): when enabled, every force evaluation first
  * computes the radial descriptors of all slots from the engine's images and lists (radius params6[3] <= list

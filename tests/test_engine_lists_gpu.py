@@ -158,21 +158,22 @@ def test_engine_lists_flag_exactly_the_dsf_exclusions():
 
 
 @pytest.mark.parametrize("tpa", [1, 32])
-def test_engine_lists_with_morton_cell_order(golden, tpa):
-    """The Morton slot order of the cells (cell_order 1) changes only where atoms sit in memory: the lists hold the
-    reference's pair set on the golden argon system and, after rebuilds inside graph runs, the oracle's pair set on
-    the positions of the last rebuild; the forces match the FP64 oracle."""
+def test_engine_lists_with_row_major_cell_order(golden, tpa):
+    """The slot order of the cells (Morton by default; row-major with cell_order 0) changes only where atoms sit in
+    memory: with row-major order too the lists hold the reference's pair set on the golden argon system and, after
+    rebuilds inside graph runs, the oracle's pair set on the positions of the last rebuild; the forces match the
+    FP64 oracle."""
     from devinproj_b200 import LennardJones, configs
     from devinproj_b200.engine import ACC, start_engine
     g = golden("argon864")
     s = _system(g)
     lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
-    eng, rlist, _ = start_engine([s], [lj], [float(g["dt"])], tpa=tpa, cell_order=1)
+    eng, rlist, _ = start_engine([s], [lj], [float(g["dt"])], tpa=tpa, cell_order=0)
     got, _, pos = engine_pairs(eng)
-    assert compare_sets(got, pair_keys(g["pair_i"], g["pair_j"], s.n), pos, s.box, rlist, f"morton tpa {tpa}") == 0
+    assert compare_sets(got, pair_keys(g["pair_i"], g["pair_j"], s.n), pos, s.box, rlist, f"row-major tpa {tpa}") == 0
     h, forces, dt = configs.argon864(seed=3)
     h.maxwell_boltzmann(300.0, np.random.default_rng(3))
-    eng, rlist, _ = start_engine([h], forces, [dt], tpa=tpa, cell_order=1)
+    eng, rlist, _ = start_engine([h], forces, [dt], tpa=tpa, cell_order=0)
     rb0 = eng.status().rebuilds
     for block in range(3):
         eng.run(41, 0, True)
@@ -181,7 +182,7 @@ def test_engine_lists_with_morton_cell_order(golden, tpa):
         st = port.State(pos, np.zeros_like(pos), h.sp.copy(), h.ids.copy(), h.box.copy(), True,
                         [("Ar", configs.AR_MASS, 0.0)])
         ref = pair_keys(*port.cell_list_pairs(st, rlist), h.n)
-        assert compare_sets(got, ref, pos, h.box, rlist, f"morton hot argon tpa {tpa} block {block}") == 0
+        assert compare_sets(got, ref, pos, h.box, rlist, f"row-major hot argon tpa {tpa} block {block}") == 0
     assert eng.status().rebuilds - rb0 >= 6
     p, v, a = eng.get_state()
     from devinproj_b200.engine import LEN
