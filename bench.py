@@ -486,6 +486,7 @@ def main():
     fp64 = None
     if args.fp64_steps > 0 and not ensemble:
         fp64 = fp64_dropin_device_resident(args, local, stream)
+    learned = learned_correction_cost(stream) if args.workload == "lj1m" and world == 1 else None
     del eng
 
     peaks, peak_kind = measured_peaks()
@@ -544,6 +545,8 @@ def main():
     if fp64 is not None:
         fp64["fp32c_over_fp64"] = (value / world) / fp64["value"]
         line["fp64_dropin_device_resident"] = fp64
+    if learned is not None:
+        line["learned_correction_cost"] = learned
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_reference()
     if rank == 0:
@@ -551,6 +554,38 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def learned_correction_cost(stream, steps=200):
+    """Step time of the 8000-ion NaCl melt (configs[3]: LJ + DSF rc 10 A) in the graph, plain and with the learned
+    DSF->Ewald correction (descriptors + tensor-core MLP) refreshed every step and every 10th step. The kernels'
+    work does not depend on the weights, so an untrained network stands in for the trained one here; the
+    correction's accuracy comes from `--experiment learned`."""
+    import torch
+
+    from devinproj_b200 import GpuSimulation, configs
+    from devinproj_b200.learned import LearnedCorrection
+    s, forces, dt = configs.nacl8000()
+    plain = GpuSimulation(s.copy(), forces, dt=dt)
+    corr = GpuSimulation(s.copy(), forces, dt=dt, correction=LearnedCorrection(seed=0), validate_every=0)
+
+    def graph_ms(engine):
+        engine.run(steps, 0, True)           # the block's graph is captured here
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        engine.run(steps, 0, True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        engine.check("learned correction timing")
+        return a.elapsed_time(b) / steps
+
+    out = {"ions": s.n, "plain_ms_per_step": graph_ms(plain.engine)}
+    for stride in (1, 10):
+        corr.engine.set_correction_stride(stride)
+        out[f"corrected_ms_per_step_stride{stride}"] = graph_ms(corr.engine)
+        out[f"overhead_stride{stride}"] = out[f"corrected_ms_per_step_stride{stride}"] / out["plain_ms_per_step"] - 1
+    return out
 
 
 def fp64_dropin_device_resident(args, local, stream):
