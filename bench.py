@@ -446,6 +446,7 @@ def main():
         slope_rel = max_over_ranks(slope_rel)
 
     # ---------------------------------------------------------------- end to end (host buffers)
+    pos_d, vel_d, _ = eng.get_state()          # the current state is the first step's input
     pos_h = (pos_d.cpu() * 1.0).pin_memory()
     vel_h = vel_d.cpu().pin_memory()
     out_p = torch.empty_like(pos_h).pin_memory()
@@ -453,30 +454,18 @@ def main():
     dev_p = torch.empty_like(pos_d)
     dev_v = torch.empty_like(vel_d)
     eng.run(1, 0, True)
-    # the velocities go back on a second stream, so that their device-to-host copy overlaps the next step's
-    # host-to-device copy of the positions (the two directions use separate copy engines)
-    side = torch.cuda.Stream()
-    v_back = torch.cuda.Event()
-    v_back.record(stream)
     torch.cuda.synchronize()
     barrier()
     w0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         dev_p.copy_(pos_h, non_blocking=True)
-        stream.wait_event(v_back)            # the last step's velocities are on the host
         dev_v.copy_(vel_h, non_blocking=True)
         eng.load_state(dev_p, dev_v)
         eng.run(1, 0, True)
         p, v, _ = eng.get_state()
-        out_p.copy_(p, non_blocking=True)    # positions first: the next step's upload starts as soon as they are back
-        got = torch.cuda.Event()
-        got.record(stream)
-        side.wait_event(got)
-        v.record_stream(side)
-        with torch.cuda.stream(side):
-            out_v.copy_(v, non_blocking=True)
-            v_back.record(side)
-        rec = eng.records(1)           # the step's energies: synchronises the main stream
+        out_p.copy_(p, non_blocking=True)
+        out_v.copy_(v, non_blocking=True)
+        rec = eng.records(1)           # the step's energies: synchronises
         pos_h, out_p = out_p, pos_h
         vel_h, out_v = out_v, vel_h
     torch.cuda.synchronize()
@@ -539,9 +528,7 @@ def main():
         "clocks": clocks,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n + 64,
                 "steps": args.e2e_steps, "path": "pinned host pos/vel -> acs_engine_load_state -> 1 step graph -> "
-                                                  "acs_engine_get_state -> pinned host + energy record (velocity "
-                                                  "read-back on a second stream, overlapping the next position "
-                                                  "upload)",
+                                                  "acs_engine_get_state -> pinned host + energy record",
                 "host_cores": host_cores},
         "gpu_launches": launches,
         "wall_s_timed": wall,
