@@ -507,6 +507,7 @@ def main():
         "config": full_config(cfg, args, world),
         "accuracy": {"force_rms_rel_err_vs_fp64": f_err,
                      "energy_drift_report_metric": drift, "energy_drift_window_steps": args.drift_steps,
+                     "energy_drift_10k": drift if args.drift_steps == 10000 else None,
                      "energy_drift_window_start_step": max(args.drift_equil,
                                                            args.warmup + 2 * args.steps + min(args.steps, 1000)) + 1,
                      "energy_drift_linear_per_step_rel": slope_rel, "energy_drift_window_ms": drift_ms,
