@@ -72,7 +72,7 @@ def _store(db):
 
 
 def candidates(n_total, nb):
-    tpas = [t for t in (1, 2, 4, 8, 16, 32) if t * 4 <= max(nb, 4)]
+    tpas = [t for t in (1, 2, 4, 8, 16, 32) if t * 2 <= max(nb, 2)]   # at least two list entries per lane
     if n_total > 2_000_000:
         tpas = [t for t in tpas if t <= 4]
     grids = [0, 4, 8]

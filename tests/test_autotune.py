@@ -29,11 +29,12 @@ def test_signature_buckets_and_distinguishes_workloads():
 
 
 def test_candidates():
-    # threads per atom: at most a quarter of the neighbours each, powers of two up to 32; step grids of one thread
+    # threads per atom: at least two list entries per lane, powers of two up to 32; step grids of one thread
     # per slot or 4 or 8 looping blocks per SM
     g = (0, 4, 8)
     assert autotune.candidates(1000, 200) == [(t, k) for t in (1, 2, 4, 8, 16, 32) for k in g]
-    assert autotune.candidates(1000, 40) == [(t, k) for t in (1, 2, 4, 8) for k in g]
+    assert autotune.candidates(1000, 78) == [(t, k) for t in (1, 2, 4, 8, 16, 32) for k in g]
+    assert autotune.candidates(1000, 40) == [(t, k) for t in (1, 2, 4, 8, 16) for k in g]
     assert autotune.candidates(1000, 1) == [(1, k) for k in g]
     # above two million atoms only 1, 2 or 4 threads per atom
     assert autotune.candidates(3_000_000, 200) == [(t, k) for t in (1, 2, 4) for k in g]
