@@ -977,18 +977,24 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   }
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(4);
-  for (int64_t r = gtid; r < E.R; r += gstride) {
+  // (b) a block per flagged replica scans its chunk totals (exclusive, from the replica's first slot)
+  for (int r = blockIdx.x; r < E.R; r += gridDim.x) {
     if (!fl[r]) continue;
     const RepDev& R = E.rep[r];
-    int64_t off = R.atom0;
-    for (int c = R.cc0; c < R.cc0 + R.ncc; ++c) {
-      const int t = E.cc_sum[c];
-      E.cc_sum[c] = (int32_t)off;
-      off += t;
+    int carry = 0;
+    for (int c0 = 0; c0 < R.ncc; c0 += blockDim.x) {
+      const int c = c0 + (int)threadIdx.x;
+      const int t = c < R.ncc ? E.cc_sum[R.cc0 + c] : 0;
+      int total;
+      const int ex = block_scan_excl(t, &total);
+      if (c < R.ncc) E.cc_sum[R.cc0 + c] = (int32_t)(R.atom0 + carry + ex);
+      carry += total;
     }
-    E.start[R.cellbase + R.ncells] = (int32_t)(R.atom0 + R.n);
-    E.flag[r] = 0;
-    atomicAdd(&E.status->rebuilds, 1);
+    if (threadIdx.x == 0) {
+      E.start[R.cellbase + R.ncells] = (int32_t)(R.atom0 + R.n);
+      E.flag[r] = 0;
+      atomicAdd(&E.status->rebuilds, 1);
+    }
   }
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(5);
