@@ -42,6 +42,7 @@ constexpr int kIdxBits = 27;
 constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
 constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
+constexpr int kSmallUnit = 4;   // atoms a warp takes at a time in the list build of one-cell-axis replicas
 
 struct RepDev {
   int64_t atom0;
@@ -115,7 +116,8 @@ struct Eng {
                                  // apply, end-half scale (records), 3 spare (8 doubles)
   double* rec_bath;              // bath energy per record and replica
   int32_t* fcell;                // per rebuild: prefix over replicas of the flagged cells the warp-per-cell
-                                 // list build covers (R + 1 entries)
+                                 // list build covers (R + 1 entries), then that build's cell counter
+  int32_t* fsmall;               // the same for the atoms of flagged one-cell-axis replicas, then a unit counter
   const int32_t* ex_start;       // DSF exclusions by atom index within a replica (CSR), or none
   const int32_t* ex_ids;
   int32_t n_ex_ids;
@@ -823,6 +825,34 @@ struct PairScan {
   }
 };
 
+// The list of atom i built by one warp: the lanes take 32 candidates at a time, in stencil order and ascending
+// slot, and a ballot keeps the accepted ones in that order.
+template <bool EX>
+__device__ __forceinline__ void list_atom_warp(const Eng& E, const RepDev& R, int64_t i, int dst, int lane) {
+  PairScan ps(E, R, i, dst);
+  int cnt = 0;
+  for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
+    for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
+      for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
+        const int cc = ps.cell(a, b, d);
+        const int k0 = E.start[E.crank[cc]], k1 = E.start[E.crank[cc] + 1];
+        for (int base = k0; base < k1; base += 32) {
+          const int k = base + lane;
+          int code = -1;
+          if (k < k1 && k != i) code = ps.test(k, a, b, d);
+          const unsigned bal = __ballot_sync(0xffffffffu, code >= 0);
+          const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (code >= 0 && pos < E.maxnb) {
+            uint32_t v = (uint32_t)k | ((uint32_t)code << kIdxBits);
+            if (EX && dsf_excluded(E, E.id[i], E.id[k])) v |= E.ex_bit;
+            ps.lst[(int64_t)pos * E.G] = (int32_t)v;
+          }
+          cnt += __popc(bal);
+        }
+      }
+  if (lane == 0) ps.finish(cnt);
+}
+
 // Exact decision for a candidate in the FP32 band around the list radius, on a replica with >= 3 cells per
 // axis: the reference's FP64 filter on the absolute positions (minimum image by comparison with box/2).
 // Kept out of line so the candidate loop branches around it instead of issuing it predicated.
@@ -888,21 +918,37 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   unsigned long long t_prev = (blockIdx.x == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
   if (blockIdx.x == 0) {
     // exclusive prefix of the cells the warp-per-cell list build visits (flagged replicas with >= 3 cells on
-    // every axis), so that its warps take only those cells, in turn (balanced when few replicas rebuild)
+    // every axis), so that its warps take only those cells (balanced when few replicas rebuild)
+    // and of the atoms of flagged replicas with a one-cell axis (the list build's warp-per-atom part)
     const int per = (E.R + blockDim.x - 1) / blockDim.x, r0 = threadIdx.x * per;
-    int sum = 0;
+    int sum = 0, sum_s = 0;
     for (int r = r0; r < min(r0 + per, E.R); ++r) {
       const RepDev& R = E.rep[r];
-      if (fl[r] && R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3) sum += R.ncells;
+      const bool cells3 = R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3;
+      if (fl[r]) {
+        if (cells3) sum += R.ncells;
+        else sum_s += R.n;
+      }
     }
-    int total;
+    int total, total_s;
     int ex = block_scan_excl(sum, &total);
+    int ex_s = block_scan_excl(sum_s, &total_s);
     for (int r = r0; r < min(r0 + per, E.R); ++r) {
       E.fcell[r] = ex;
+      E.fsmall[r] = ex_s;
       const RepDev& R = E.rep[r];
-      if (fl[r] && R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3) ex += R.ncells;
+      const bool cells3 = R.nc[0] >= 3 && R.nc[1] >= 3 && R.nc[2] >= 3;
+      if (fl[r]) {
+        if (cells3) ex += R.ncells;
+        else ex_s += R.n;
+      }
     }
-    if (threadIdx.x == 0) E.fcell[E.R] = total;
+    if (threadIdx.x == 0) {
+      E.fcell[E.R] = total;
+      E.fcell[E.R + 1] = 0;   // the list build's cell counter
+      E.fsmall[E.R] = total_s;
+      E.fsmall[E.R + 1] = 0;  // and its atom-unit counter
+    }
   }
 #define PHASE(k)                                                  \
   if (blockIdx.x == 0 && threadIdx.x == 0) {                      \
@@ -1087,32 +1133,11 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       if (!fl[r]) continue;
       const RepDev& R = E.rep[r];
       if (i - R.atom0 >= R.n) continue;
-      PairScan ps(E, R, i, dst);
-      int cnt = 0;
-      for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
-        for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
-          for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
-            const int cc = ps.cell(a, b, d);
-            const int k0 = E.start[E.crank[cc]], k1 = E.start[E.crank[cc] + 1];
-            for (int base = k0; base < k1; base += 32) {
-              const int k = base + lane;
-              int code = -1;
-              if (k < k1 && k != i) code = ps.test(k, a, b, d);
-              const unsigned bal = __ballot_sync(0xffffffffu, code >= 0);
-              const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-              if (code >= 0 && pos < E.maxnb) {
-                uint32_t v = (uint32_t)k | ((uint32_t)code << kIdxBits);
-                if (EX && dsf_excluded(E, E.id[i], E.id[k])) v |= E.ex_bit;
-                ps.lst[(int64_t)pos * E.G] = (int32_t)v;
-              }
-              cnt += __popc(bal);
-            }
-          }
-      if (lane == 0) ps.finish(cnt);
+      list_atom_warp<EX>(E, R, i, dst, lane);
     }
   } else {
-    // Replicas with >= 3 cells on every axis: a warp per home cell (the warps take the flagged replicas' cells
-    // in turn, through the prefix block 0 wrote at the start). The candidates of the 27 stencil cells, in
+    // Replicas with >= 3 cells on every axis: a warp per home cell (a warp takes the next of the flagged
+    // replicas' cells from a counter, through the prefix block 0 wrote at the start). The candidates of the 27 stencil cells, in
     // list order (stencil cell, then ascending slot), are read 32 at a time with the cell pair's image shift
     // already added; those whose distance to the home cell's box exceeds the list radius (with the band
     // margin) cannot pair with any home atom and are dropped, the rest are compacted in order into a
@@ -1124,11 +1149,17 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     __shared__ float4 bufp[8][64];
     __shared__ uint32_t bufk[8][64];
     __shared__ int selfpos[8][32];
-    const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int nflag = __ldcg(E.fcell + E.R);   // written by block 0 in this launch: read through L2
-    for (int f = (int)gw; f < nflag; f += (int)nw) {
+    // each warp takes the next flagged cell from a counter (cleared by block 0 with the prefix), so warps that
+    // drew cheap cells take more: cell costs vary several-fold (occupancy, cell edge per replica)
+    auto next_cell = [&]() {
+      int v = 0;
+      if (lane == 0) v = atomicAdd(E.fcell + E.R + 1, 1);
+      return __shfl_sync(0xffffffffu, v, 0);
+    };
+    for (int f = next_cell(); f < nflag; f = next_cell()) {
       int r = 0;   // the replica whose range of the prefix holds f: the last r with fcell[r] <= f
       for (int lo = 0, hi = E.R - 1; lo <= hi;) {
         const int mid = (lo + hi) >> 1;
@@ -1292,40 +1323,32 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         }
       }
     }
-    // Replicas with a one-cell axis (small boxes): a thread per atom with the per-axis wrap.
-    for (int64_t i = gtid; i < E.S; i += gstride) {
-      const int r = E.tile_rep[i >> 5];
-      if (!fl[r]) continue;
-      const RepDev& R = E.rep[r];
-      if (i - R.atom0 >= R.n || !(R.nc[0] < 3 || R.nc[1] < 3 || R.nc[2] < 3)) continue;
-      PairScan ps(E, R, i, dst);
-      int cnt = 0;
-      for (int a = ps.lo[0]; a <= ps.hi[0]; ++a)
-        for (int b = ps.lo[1]; b <= ps.hi[1]; ++b)
-          for (int d = ps.lo[2]; d <= ps.hi[2]; ++d) {
-            if (ps.cell_beyond(a, b, d)) continue;
-            const int cc = ps.cell(a, b, d);
-            const int k0 = E.start[E.crank[cc]], k1 = E.start[E.crank[cc] + 1];
-            for (int k = k0; k < k1; k += 4) {
-              float q[4];
-              ps.screen4(k, k1, a, b, d, q);
-#pragma unroll
-              for (int t = 0; t < 4; ++t) {
-                if (k + t < k1 && k + t != i && q[t] < ps.hi_f) {
-                  const int code = q[t] <= ps.lo_f && !ps.any_one ? ps.scode(a, b, d) : ps.test(k + t, a, b, d);
-                  if (code >= 0) {
-                    if (cnt < E.maxnb) {
-                      uint32_t v = (uint32_t)(k + t) | ((uint32_t)code << kIdxBits);
-                      if (EX && dsf_excluded(E, E.id[i], E.id[k + t])) v |= E.ex_bit;
-                      ps.lst[(int64_t)cnt * E.G] = (int32_t)v;
-                    }
-                    ++cnt;
-                  }
-                }
-              }
-            }
-          }
-      ps.finish(cnt);
+    // Replicas with a one-cell axis (small boxes, cells of the whole edge): a warp per atom, the per-axis wrap in
+    // the pair test. Warps take units of kSmallUnit atoms in turn from a counter, through a prefix of the flagged
+    // small replicas' atom counts that block 0 wrote at the start.
+    const int nsmall = __ldcg(E.fsmall + E.R);
+    auto next_unit = [&]() {
+      int v = 0;
+      if (lane == 0) v = atomicAdd(E.fsmall + E.R + 1, 1);
+      return __shfl_sync(0xffffffffu, v, 0);
+    };
+    for (int u = next_unit(); u < (nsmall + kSmallUnit - 1) / kSmallUnit; u = next_unit()) {
+      const int q0 = u * kSmallUnit, q1 = min(q0 + kSmallUnit, nsmall);
+      int r = 0;   // the last r with fsmall[r] <= q0: the replica that holds atom q0 of the prefix
+      for (int lo = 0, hi = E.R - 1; lo <= hi;) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldcg(E.fsmall + mid) <= q0) {
+          r = mid;
+          lo = mid + 1;
+        } else {
+          hi = mid - 1;
+        }
+      }
+      for (int q = q0; q < q1; ++q) {
+        while (r + 1 < E.R && __ldcg(E.fsmall + r + 1) <= q) ++r;
+        const RepDev& R = E.rep[r];
+        list_atom_warp<EX>(E, R, R.atom0 + (q - __ldcg(E.fsmall + r)), dst, lane);
+      }
     }
   }
   __syncthreads();
@@ -1794,11 +1817,12 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(8 * (size_t)NCH);                    // 44 Nose-Hoover chunk partials
   L.add(8 * 8 * (size_t)R);                  // 45 Nose-Hoover state
   L.add(8 * (size_t)rec_cap * R);            // 46 bath-energy records
-  L.add(4 * ((size_t)R + 1));                // 47 flagged-cell prefix of a rebuild
+  L.add(4 * ((size_t)R + 2));                // 47 flagged-cell prefix of a rebuild, list-build cell counter
   L.add(4 * ((size_t)n_ex_ids + 1));         // 48 DSF exclusions: CSR starts by atom id
   L.add(4 * ((size_t)n_ex + 1));             // 49 DSF exclusions: excluded ids
   L.add(4 * (size_t)C);                      // 50 crank (cell id -> slot-order position)
   L.add(4 * (size_t)C);                      // 51 cell_at (position -> cell id)
+  L.add(4 * ((size_t)R + 2));                // 52 flagged one-cell-axis atoms prefix, list-build unit counter
   return L;
 }
 
@@ -2081,6 +2105,7 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.ex_ids = (const int32_t*)(b + L.off[49]);
   E.crank = (int32_t*)(b + L.off[50]);
   E.cell_at = (int32_t*)(b + L.off[51]);
+  E.fsmall = (int32_t*)(b + L.off[52]);
   E.ex_bit = cfg->n_ex_ids > 0 ? kExBit : 0u;
   E.jmask = cfg->n_ex_ids > 0 ? kExBit - 1u : kIdxMask;
   E.thermo = cfg->thermo.kind;
