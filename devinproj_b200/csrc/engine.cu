@@ -43,6 +43,7 @@ constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
 constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
 constexpr int kSmallUnit = 4;   // atoms a warp takes at a time in the list build of one-cell-axis replicas
+constexpr int kSkipU = 8;       // grid strides whose replica indices a rebuild phase loads together
 
 struct RepDev {
   int64_t atom0;
@@ -825,6 +826,28 @@ struct PairScan {
   }
 };
 
+// Grid-stride walk over the slots of flagged replicas (padding slots excluded), calling f(s, r). The replica
+// indices of kSkipU strides are loaded together, so skipping the slots of unflagged replicas costs one memory
+// round trip per kSkipU strides instead of one per stride (an ensemble rebuild touches a few % of its slots).
+template <class FL, class F>
+__device__ __forceinline__ void for_flagged_slots(const Eng& E, const FL& fl, int64_t gtid, int64_t gstride, F&& f) {
+  for (int64_t s0 = gtid; s0 < E.S; s0 += kSkipU * gstride) {
+    unsigned m = 0u;
+#pragma unroll
+    for (int u = 0; u < kSkipU; ++u) {
+      const int64_t s = s0 + u * gstride;
+      if (s < E.S && fl[__ldg(E.tile_rep + (s >> 5))]) m |= 1u << u;
+    }
+    while (m) {
+      const int u = __ffs(m) - 1;
+      m &= m - 1u;
+      const int64_t s = s0 + u * gstride;
+      const int r = __ldg(E.tile_rep + (s >> 5));
+      if (s - E.rep[r].atom0 < E.rep[r].n) f(s, r);
+    }
+  }
+}
+
 // The list of atom i built by one warp: the lanes take 32 candidates at a time, in stencil order and ascending
 // slot, and a ballot keeps the accepted ones in that order.
 template <bool EX>
@@ -969,11 +992,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(2);
   // P1: absolute wrapped positions and new cells
-  for (int64_t s = gtid; s < E.S; s += gstride) {
-    const int r = E.tile_rep[s >> 5];
-    if (!fl[r]) continue;
+  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t s, int r) {
     const RepDev& R = E.rep[r];
-    if (s - R.atom0 >= R.n) continue;
     int c0, c1, c2;
     cell_coords(E.cellid[s] - R.cellbase, R, c0, c1, c2);
     const double o[3] = {c0 * R.cs[0], c1 * R.cs[1], c2 * R.cs[2]};
@@ -996,7 +1016,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     const int c = R.cellbase + (nc3[0] * R.nc[1] + nc3[1]) * R.nc[2] + nc3[2];
     E.newcell[s] = c;
     atomicAdd(&E.count[c], 1);
-  }
+  });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(3);
   // P2: exclusive scan of cell counts -> slot starts, in fixed 1024-cell chunks: (a) chunk-local scans,
@@ -1052,31 +1072,25 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(6);
   // P3: scatter old slots to new slots
-  for (int64_t s = gtid; s < E.S; s += gstride) {
-    const int r = E.tile_rep[s >> 5];
-    if (!fl[r] || s - E.rep[r].atom0 >= E.rep[r].n) continue;
+  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t s, int) {
     const int c = E.newcell[s];
     E.perm[E.start[E.crank[c]] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
-  }
+  });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(7);
   // P3b: deterministic order inside each cell: every atom's rank among its cell's atoms by old slot
-  for (int64_t k = gtid; k < E.S; k += gstride) {
-    const int r = E.tile_rep[k >> 5];
-    if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
+  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int) {
     const int v = E.perm[k];
     const int c = E.newcell[v];
     const int a0 = E.start[E.crank[c]], a1 = E.start[E.crank[c] + 1];
     int rank = 0;
     for (int a = a0; a < a1; ++a) rank += (E.perm[a] < v);
     E.perm2[a0 + rank] = v;
-  }
+  });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(8);
   // P4: gather into new order
-  for (int64_t k = gtid; k < E.S; k += gstride) {
-    const int r = E.tile_rep[k >> 5];
-    if (!fl[r] || k - E.rep[r].atom0 >= E.rep[r].n) continue;
+  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int) {
     const int o = E.perm2[k];
     E.tmp_cell[k] = E.newcell[o];
     E.tmp_id[k] = E.id[o];
@@ -1086,15 +1100,12 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       E.tmp_xa[3 * k + d] = E.xa[3 * o + d];
       E.tmp_v[3 * k + d] = E.v[3 * o + d];
     }
-  }
+  });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(9);
   // P5: commit; offsets from the new cell origins; images
-  for (int64_t k = gtid; k < E.S; k += gstride) {
-    const int r = E.tile_rep[k >> 5];
-    if (!fl[r]) continue;
+  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int r) {
     const RepDev& R = E.rep[r];
-    if (k - R.atom0 >= R.n) continue;
     const int c = E.tmp_cell[k];
     int c0, c1, c2;
     cell_coords(c - R.cellbase, R, c0, c1, c2);
@@ -1113,7 +1124,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
 #pragma unroll
     for (int d = 0; d < 3; ++d) E.v[3 * k + d] = E.tmp_v[3 * k + d];
     E.img[dst][k] = make_img(ux, uy, uz, E.tmp_sp[k]);
-  }
+  });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(10);
   // P6: neighbour lists in one pass over the 27-cell stencil. Each candidate's r^2 is first computed in
