@@ -152,7 +152,8 @@ def test_engine_lj_species_without_parameters_do_not_interact():
 def test_engine_orthorhombic_boxes(nz, tpa):
     """Boxes with unequal edges: an LJ fluid on a perturbed 28 x 19 x nz lattice (spacing 1.06 sigma; box 29.7
     x 20.1 x 6.4 sigma has a one-cell axis, 12.7 sigma does not), engine vs the FP64 plug-in at the start and
-    after 100 steps, through the thread-per-atom (one-cell axis), warp-per-atom and warp-per-cell list builds."""
+    after 100 steps, through the list builds for a one-cell axis (a warp per atom), for >= 8 threads per atom (a
+    warp per atom) and for >= 3 cells per axis (a warp per cell)."""
     from accusim import System
     from devinproj_b200 import GpuSimulation, LennardJones, configs
     rng = np.random.default_rng(nz + tpa)

@@ -191,3 +191,52 @@ def test_engine_lists_with_row_major_cell_order(golden, tpa):
     Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(st)
     F = a.cpu().numpy() * ACC * configs.AR_MASS
     assert float(np.sqrt(np.mean(np.sum((F - Fo) ** 2, 1)) / np.mean(np.sum(Fo ** 2, 1)))) <= 1e-5
+
+
+@pytest.mark.parametrize("tpa", [1, 32])
+def test_engine_lists_with_a_one_cell_axis(tpa):
+    """A box with a one-cell axis (29.7 x 20.1 x 6.4 sigma: 6.4 sigma is under three list radii, so that axis has
+    one cell and the pair test wraps it), in one engine with a replica that has >= 3 cells per axis: the lists of
+    both equal the oracle's pair search at the list radius on the positions of the last rebuild, at the start and
+    after rebuilds inside graph runs."""
+    from accusim import System
+    from devinproj_b200 import LennardJones, configs
+    from devinproj_b200.engine import LEN, start_engine
+    rng = np.random.default_rng(7)
+    a = 1.06 * configs.AR_SIGMA
+    systems = []
+    for n in (np.array([28, 19, 6]), np.array([12, 12, 12])):
+        s = System(3, box=n * a, periodic=True)
+        s.add_species("Ar", configs.AR_MASS)
+        g = np.stack(np.meshgrid(*[np.arange(k) for k in n], indexing="ij"), -1).reshape(-1, 3)
+        s.add("Ar", ((g + 0.5) * a + rng.normal(0, 0.05 * configs.AR_SIGMA, g.shape)) % s.box)
+        s.maxwell_boltzmann(300.0, rng)
+        systems.append(s)
+    lj = LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5)
+    eng, rlist, _ = start_engine([x.copy() for x in systems], [lj], [5e-15, 5e-15], tpa=tpa)
+    assert 6 * a < 3 * rlist < 12 * a
+    rb0 = eng.status().rebuilds
+    for block in range(4):
+        if block:
+            eng.run(29, 0, True)
+            eng.check("run")
+        keys, pos = eng.list_entries()
+        keys = keys.cpu().numpy()
+        pos = pos.cpu().numpy() * LEN
+        n_all = int(eng.offsets[-1])
+        ex = keys >> 1
+        i, j = ex // n_all, ex % n_all
+        assert np.all(keys >= 0) and not np.any(i == j)
+        for r, s in enumerate(systems):
+            o0, o1 = int(eng.offsets[r]), int(eng.offsets[r + 1])
+            sel = (i >= o0) & (i < o1) & (i < j)
+            assert np.all((j[sel] >= o0) & (j[sel] < o1)), "an entry names another replica's atom"
+            got = np.sort((i[sel] - o0) * s.n + (j[sel] - o0))
+            back = (j >= o0) & (j < o1) & (i > j)
+            assert np.array_equal(got, np.sort((j[back] - o0) * s.n + (i[back] - o0))), "not listed both ways"
+            p = pos[o0:o1]
+            st = port.State(p, np.zeros_like(p), s.sp.copy(), s.ids.copy(), s.box.copy(), True,
+                            [("Ar", configs.AR_MASS, 0.0)])
+            ref = pair_keys(*port.cell_list_pairs(st, rlist), s.n)
+            assert compare_sets(got, ref, p, s.box, rlist, f"replica {r} tpa {tpa} block {block}") == 0
+    assert eng.status().rebuilds - rb0 >= 4
