@@ -731,7 +731,7 @@ struct PairScan {
   const RepDev& R;
   int64_t i;
   int c[3], lo[3], hi[3];
-  bool one[3], any_one;
+  bool one[3];
   float4 pi;
   float lo_f, hi_f, Lf[3];
   const float4* im;
@@ -744,11 +744,9 @@ struct PairScan {
     const float rl2f = (float)R.rl2;
     lo_f = rl2f * (1.0f - 1e-4f);
     hi_f = rl2f * (1.0f + 1e-4f);
-    any_one = false;
     for (int d = 0; d < 3; ++d) {
       Lf[d] = (float)R.L[d];
       one[d] = R.nc[d] < 3;
-      any_one |= one[d];
       lo[d] = one[d] ? 0 : -1;
       hi[d] = one[d] ? 0 : 1;
     }
@@ -757,37 +755,6 @@ struct PairScan {
   __device__ int cell(int a, int b, int d) const {
     const int n0 = wrapc(c[0] + a, R.nc[0]), n1 = wrapc(c[1] + b, R.nc[1]), n2 = wrapc(c[2] + d, R.nc[2]);
     return R.cellbase + (n0 * R.nc[1] + n1) * R.nc[2] + n2;
-  }
-  __device__ static int scode(int a, int b, int d) { return (a + 1) + 3 * (b + 1) + 9 * (d + 1); }
-  // lower bound of the distance^2 from atom i to the neighbour cell's box, beyond the list radius?
-  __device__ bool cell_beyond(int a, int b, int d) const {
-    const float p[3] = {pi.x, pi.y, pi.z};
-    const int o[3] = {a, b, d};
-    float g2 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      if (one[k] || o[k] == 0) continue;
-      const float gap = o[k] < 0 ? p[k] : R.csf[k] - p[k];
-      g2 += gap > 0.f ? gap * gap : 0.f;
-    }
-    return g2 > hi_f;
-  }
-  // FP32 r^2 of up to four consecutive candidates (stencil cells only; no per-axis wrap needed)
-  __device__ void screen4(int k, int k1, int a, int b, int d, float q[4]) const {
-    const float sa = a * R.csf[0], sb = b * R.csf[1], sd = d * R.csf[2];
-    float4 pj[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) pj[t] = im[min(k + t, k1 - 1)];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      float x = (pj[t].x - pi.x) + sa, y = (pj[t].y - pi.y) + sb, z = (pj[t].z - pi.z) + sd;
-      if (any_one) {
-        if (one[0]) x -= x > 0.5f * Lf[0] ? Lf[0] : (x < -0.5f * Lf[0] ? -Lf[0] : 0.f);
-        if (one[1]) y -= y > 0.5f * Lf[1] ? Lf[1] : (y < -0.5f * Lf[1] ? -Lf[1] : 0.f);
-        if (one[2]) z -= z > 0.5f * Lf[2] ? Lf[2] : (z < -0.5f * Lf[2] ? -Lf[2] : 0.f);
-      }
-      q[t] = x * x + y * y + z * z;
-    }
   }
   // Exact decision for candidate k: the code to store, or -1. Band candidates use the FP64 filter; others
   // are decided by the FP32 screen (with the FP32 wrap for one-cell axes).
@@ -1134,8 +1101,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   // which for every pair that can lie inside the list radius (< box/2) is the IEEE result of
   // d - box*round(d/box). The image shift stored with j is the stencil offset (>= 3 cells per edge) or
   // minus the wrap (1 cell per edge). Entries are in stencil order, ascending slot within a cell, however
-  // the work is split: a warp per atom when the pair kernel runs >= 8 threads per atom (small systems),
-  // else a thread per atom that skips neighbour cells whose box lies beyond the list radius.
+  // the work is split: a warp per atom when the pair kernel runs >= 8 threads per atom (small systems), else a
+  // warp per home cell, and a warp per atom for replicas with a one-cell axis.
   if (E.tpa >= 8) {
     const int64_t gw = gtid >> 5, nw = gstride >> 5;
     const int lane = threadIdx.x & 31;
