@@ -9,7 +9,8 @@ Inputs (positions, velocities, 400+ MB of neighbour lists) exceed the 126 MB L2,
 Under torchrun each rank advances its own independent system (replicas only; no collective in the step
 loop), or, for the replica ensemble, its shard of the replicas; rank 0 prints one JSON line. The line also
 carries the energy drift of a fixed 10^4-step window and the throughput of the plain FP64 plug-ins running
-device-resident inside accusim's own Simulation.run (the denominator of the FP32c path's speed-up).
+device-resident inside accusim's own Simulation.run (the denominator of the FP32c path's speed-up), and, for
+the 1M-atom workload, the learned DSF->Ewald correction's step overhead and held-out accuracy (8000-ion melt).
 `--impl reference` times the unmodified reference (accusim, installed under baseline/_ref) on this host's
 cores (all of them, one process each) for the same metric.
 """
@@ -263,6 +264,9 @@ def main():
                     help="steps of the plain FP64 plug-ins (device-resident GpuSystem in accusim's Simulation.run) "
                          "timed for the speed-up denominator; 0 skips them")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned-snapshots", type=int, default=2000,
+                    help="1M-atom line only: snapshots of the learned correction's held-out accuracy leg (8000-ion "
+                         "melt, ~45 s); 0 skips it")
     ap.add_argument("--cell-order", type=int, default=1, choices=[0, 1],
                     help="slot order of the cells: 1 Morton (default), 0 row-major")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
@@ -481,6 +485,8 @@ def main():
     if args.fp64_steps > 0 and not ensemble:
         fp64 = fp64_dropin_device_resident(args, local, stream)
     learned = learned_correction_cost(stream) if args.workload == "lj1m" and world == 1 else None
+    learned_acc = (learned_correction_accuracy(args.learned_snapshots)
+                   if args.workload == "lj1m" and world == 1 and args.learned_snapshots > 0 else None)
     del eng
 
     peaks, peak_kind = measured_peaks()
@@ -544,6 +550,8 @@ def main():
         line["fp64_dropin_device_resident"] = fp64
     if learned is not None:
         line["learned_correction_cost"] = learned
+    if learned_acc is not None:
+        line["learned_correction_accuracy"] = learned_acc
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_reference()
     if rank == 0:
@@ -557,7 +565,7 @@ def learned_correction_cost(stream, steps=200):
     """Step time of the 8000-ion NaCl melt (configs[3]: LJ + DSF rc 10 A) in the graph, plain and with the learned
     DSF->Ewald correction (descriptors + tensor-core MLP) refreshed every step and every 10th step. The kernels'
     work does not depend on the weights, so an untrained network stands in for the trained one here; the
-    correction's accuracy comes from `--experiment learned`."""
+    correction's accuracy is the separate held-out leg (`learned_correction_accuracy`)."""
     import torch
 
     from devinproj_b200 import GpuSimulation, configs
@@ -583,6 +591,31 @@ def learned_correction_cost(stream, steps=200):
         out[f"corrected_ms_per_step_stride{stride}"] = graph_ms(corr.engine)
         out[f"overhead_stride{stride}"] = out[f"corrected_ms_per_step_stride{stride}"] / out["plain_ms_per_step"] - 1
     return out
+
+
+def learned_correction_accuracy(snapshots, epochs=20, lr=2e-3):
+    """Held-out accuracy of the learned DSF->Ewald correction on the 8000-ion melt, the same recipe
+    as `--experiment learned` with one training setting: `snapshots` seeded snapshots (Langevin melt at 4000 K,
+    cooled to 1300 K, sampled every 20 NVE steps, labels device Ewald minus FP64 DSF), trained on the first 90%
+    and scored on the last 10%, which training never sees (RMS relative force error against Ewald)."""
+    import numpy as np
+    import torch
+
+    from devinproj_b200.learned import LearnedCorrection, generate_dataset
+    t0 = time.perf_counter()
+    d = generate_dataset(snapshots, seed=0, n_sites=20, verbose=False)
+    t_gen = time.perf_counter() - t0
+    n_train = int(0.9 * snapshots)
+    t0 = time.perf_counter()
+    lc = LearnedCorrection(seed=0)
+    hist = lc.train(d, np.arange(n_train), epochs=epochs, batch_tiles=64, lr=lr)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    e_dsf, e_corr = lc.errors(d, np.arange(n_train, snapshots))
+    return {"ions": 8000, "snapshots": snapshots, "train_snapshots": n_train, "heldout_snapshots": snapshots - n_train,
+            "epochs": epochs, "lr": lr, "train_loss_first_last": [hist[0], hist[-1]],
+            "heldout_rms_rel_err_dsf": e_dsf, "heldout_rms_rel_err_corrected": e_corr, "error_ratio": e_dsf / e_corr,
+            "dataset_s": t_gen, "train_s": t_train}
 
 
 def fp64_dropin_device_resident(args, local, stream):
