@@ -1484,6 +1484,7 @@ __global__ void __launch_bounds__(256, 4) k_desc_engine(Eng E, int src, DescP P,
   constexpr int kU = 4;
   __shared__ float4 stage[8][32 * kU];   // (dx/r, dy/r, dz/r, r) per neighbour
   __shared__ float stage2[8][32 * kU];   // log2(fc)
+  __shared__ float4 shift_tab[8][27];    // image shift of each stencil code, this warp's replica
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= E.S) return;
@@ -1499,6 +1500,10 @@ __global__ void __launch_bounds__(256, 4) k_desc_engine(Eng E, int src, DescP P,
     const float mu = P.r0 + lane * P.dmu;
     const int m = E.nnb[i];
     const int32_t* lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
+    if (lane < 27)
+      shift_tab[wib][lane] = make_float4((lane % 3 - 1) * R.csf[0], ((lane / 3) % 3 - 1) * R.csf[1],
+                                         (lane / 9 - 1) * R.csf[2], 0.f);
+    __syncwarp();
     for (int base = 0; base < m; base += 32 * kU) {
       uint32_t e[kU];
 #pragma unroll
@@ -1517,10 +1522,10 @@ __global__ void __launch_bounds__(256, 4) k_desc_engine(Eng E, int src, DescP P,
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
         const int k = base + 32 * u + lane;
-        const uint32_t code = e[u] >> kIdxBits;
-        const float fx = (pj[u].x - pi.x) + ((int)(code % 3) - 1) * R.csf[0];
-        const float fy = (pj[u].y - pi.y) + ((int)((code / 3) % 3) - 1) * R.csf[1];
-        const float fz = (pj[u].z - pi.z) + ((int)(code / 9) - 1) * R.csf[2];
+        const float4 sh = shift_tab[wib][e[u] >> kIdxBits];
+        const float fx = (pj[u].x - pi.x) + sh.x;
+        const float fy = (pj[u].y - pi.y) + sh.y;
+        const float fz = (pj[u].z - pi.z) + sh.z;
         const float r2 = fx * fx + fy * fy + fz * fz;
         const bool inside = k < m && r2 < P.rc2;
         const bool s1 = (__float_as_int(pj[u].w) & 1) != 0;
