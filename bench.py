@@ -562,7 +562,7 @@ def main():
 
 
 def learned_correction_cost(stream, steps=200):
-    """Step time of the 8000-ion NaCl melt (configs[3]: LJ + DSF rc 10 A) in the graph, plain and with the learned
+    """Step time of the 8000-ion NaCl melt (LJ + DSF, rc 10 A) in the graph, plain and with the learned
     DSF->Ewald correction (descriptors + tensor-core MLP) refreshed every step and every 10th step. The kernels'
     work does not depend on the weights, so an untrained network stands in for the trained one here; the
     correction's accuracy is the separate held-out leg (`learned_correction_accuracy`)."""
@@ -594,7 +594,7 @@ def learned_correction_cost(stream, steps=200):
 
 
 def learned_correction_accuracy(snapshots, epochs=20, lr=2e-3):
-    """Held-out accuracy of the learned DSF->Ewald correction on the 8000-ion melt, the same recipe
+    """Held-out accuracy of the learned DSF->Ewald correction on the 8000-ion NaCl melt, the same recipe
     as `--experiment learned` with one training setting: `snapshots` seeded snapshots (Langevin melt at 4000 K,
     cooled to 1300 K, sampled every 20 NVE steps, labels device Ewald minus FP64 DSF), trained on the first 90%
     and scored on the last 10%, which training never sees (RMS relative force error against Ewald)."""
