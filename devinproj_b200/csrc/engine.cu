@@ -241,8 +241,10 @@ __device__ bool grid_sync(unsigned int* bar, acs_dev_status* st, long long limit
       atomicAdd(bar + 1, 1u);
     } else {
       long long it = 0;
+      volatile int32_t* vflags = &st->flags;
       while (*vgen == gen) {
-        if (it++ >= limit) {
+        // give up after `limit` polls, or as soon as another block has given up at an earlier barrier
+        if (it++ >= limit || ((it & 255) == 0 && (*vflags & ACS_FLAG_TIMEOUT))) {
           atomicOr(&st->flags, ACS_FLAG_TIMEOUT);
           ok = 0;
           break;
