@@ -372,8 +372,11 @@ __device__ __forceinline__ void drift_or_baoab(const Eng& E, const RepDev& R, in
 // TH: 0 VelocityVerlet, 1 Langevin BAOAB (the drift of MODE 0 becomes A-O-A), 2 Nose-Hoover (MODE 0 stops
 // after the second kick like MODE 1: the thermostat's global kinetic-energy sum comes first; every mode
 // writes the group's sum of m v^2 to nh_part).
-template <bool LJ, bool DSF, bool REC, int MODE, bool ONE, int TH = 0>
-__global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int dst, unsigned ostep) {
+// PIPE: gathers one block of four entries ahead and list loads two ahead, for step grids under one wave (small
+// systems), where occupancy is set by the grid and the extra registers cost nothing; the pair terms are summed
+// in the same order, so the results are the same bit for bit.
+template <bool LJ, bool DSF, bool REC, int MODE, bool ONE, int TH = 0, bool PIPE = false>
+__global__ void __launch_bounds__(256, PIPE ? 1 : 4) k_step(Eng E, FFDev ff, int src, int dst, unsigned ostep) {
   __shared__ float4 shift_tab[8][27];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
@@ -421,10 +424,19 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
       const int n_it = m > phase ? (m - phase + tpa - 1) / tpa : 0;  // this lane's share of the list
       const int32_t* __restrict__ lst = E.nbr + (int64_t)w * E.maxnb * G + lane;  // entry phase + t*tpa at t*32
       const int n4 = n_it & ~3;
-      uint32_t en[4] = {0u, 0u, 0u, 0u};
+      uint32_t en[4] = {0u, 0u, 0u, 0u}, en2[4] = {0u, 0u, 0u, 0u};
+      float4 pjn[4];
       if (n4 > 0) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + q * 32);
+        if (PIPE) {
+          if (n4 > 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) en2[q] = (uint32_t)ld_list(lst + (4 + q) * 32);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) pjn[q] = __ldg(imgs + (en[q] & jm));
+        }
       }
       int t = 0;
       for (; t < n4; t += 4) {
@@ -432,11 +444,28 @@ __global__ void __launch_bounds__(256, 4) k_step(Eng E, FFDev ff, int src, int d
         float4 pj[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) e[q] = en[q];
+        if (PIPE) {
+          // this block's gathers were issued one block ago; issue the next block's (its entries arrived one
+          // block ago) and the list entries of the block after it
 #pragma unroll
-        for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & jm));
-        if (t + 4 < n4) {
+          for (int q = 0; q < 4; ++q) pj[q] = pjn[q];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + (t + 4 + q) * 32);
+          for (int q = 0; q < 4; ++q) en[q] = en2[q];
+          if (t + 4 < n4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) pjn[q] = __ldg(imgs + (en[q] & jm));
+          }
+          if (t + 8 < n4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) en2[q] = (uint32_t)ld_list(lst + (t + 8 + q) * 32);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) pj[q] = __ldg(imgs + (e[q] & jm));
+          if (t + 4 < n4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) en[q] = (uint32_t)ld_list(lst + (t + 4 + q) * 32);
+          }
         }
         // the four pair forces are summed in FP32, the block sum enters the Kahan sums
         float bx = 0.f, by = 0.f, bz = 0.f, bcx, bcy, bcz;
@@ -1594,6 +1623,7 @@ struct acs_engine {
   int coop_blocks = 0;
   int step_blocks = 0;
   int step_threads = 256;
+  bool pipe = false;   // plain steps with gathers one block ahead (step grids under one wave)
   int n_lj = 0, n_dsf = 0;
   std::map<long long, cudaGraphExec_t> graphs;
   int dev = 0;
@@ -1884,6 +1914,7 @@ int launch_step_t(acs_engine* e, int rec, int mode, int src, int dst, unsigned o
       else k_step<LJ, DSF, false, 0, ONE, 2><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
     } else {
       if (rec) k_step<LJ, DSF, true, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
+      else if (e->pipe) k_step<LJ, DSF, false, 0, ONE, 0, true><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
       else k_step<LJ, DSF, false, 0, ONE><<<g, b, 0, s>>>(e->E, e->ff, src, dst, ostep);
     }
   } else if (mode == 1) {
@@ -2191,6 +2222,10 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   const int64_t need = (S / G * 32 + e->step_threads - 1) / e->step_threads;
   e->step_blocks = (int)(grid_mult ? std::min<int64_t>(need, (int64_t)sms * grid_mult) : need);
   if (e->step_blocks < 1) e->step_blocks = 1;
+  // under half a wave (16 warps per SM; the step kernel holds 32 at its 64 registers) the grid, not the registers,
+  // sets the occupancy: the plain steps then take the variant with deeper load pipelining (up to 112 registers,
+  // 16 warps per SM, so still one wave)
+  e->pipe = (int64_t)e->step_blocks * e->step_threads / 32 <= 16 * (int64_t)sms;
   *out = e;
   return ACS_OK;
 }
