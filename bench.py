@@ -483,9 +483,9 @@ def main():
     # ---------------------------------------------------------------- the plain FP64 GPU drop-in
     fp64 = None
     if args.fp64_steps > 0 and not ensemble:
-        fp64 = fp64_dropin_device_resident(args, local, stream)
-    learned = learned_correction_cost(stream) if args.workload == "lj1m" and world == 1 else None
-    learned_acc = (learned_correction_accuracy(args.learned_snapshots)
+        fp64 = secondary_leg(fp64_dropin_device_resident, args, local, stream)
+    learned = secondary_leg(learned_correction_cost, stream) if args.workload == "lj1m" and world == 1 else None
+    learned_acc = (secondary_leg(learned_correction_accuracy, args.learned_snapshots)
                    if args.workload == "lj1m" and world == 1 and args.learned_snapshots > 0 else None)
     del eng
 
@@ -545,7 +545,7 @@ def main():
         line["sharding"] = {"replicas": len(shard) if world == 1 else None, "replicas_total": 768,
                             "this_rank_replicas": len(shard), "this_rank_atoms": n, "atoms_total": n_global,
                             "rule": "largest replica first to the least-loaded rank; no collective while stepping"}
-    if fp64 is not None:
+    if fp64 is not None and "value" in fp64:
         fp64["fp32c_over_fp64"] = (value / world) / fp64["value"]
         line["fp64_dropin_device_resident"] = fp64
     if learned is not None:
@@ -553,7 +553,7 @@ def main():
     if learned_acc is not None:
         line["learned_correction_accuracy"] = learned_acc
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_reference()
+        line["cpu_baseline"] = secondary_leg(cpu_baseline_reference)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -591,6 +591,17 @@ def learned_correction_cost(stream, steps=200):
         out[f"corrected_ms_per_step_stride{stride}"] = graph_ms(corr.engine)
         out[f"overhead_stride{stride}"] = out[f"corrected_ms_per_step_stride{stride}"] / out["plain_ms_per_step"] - 1
     return out
+
+
+def secondary_leg(fn, *args):
+    """One of the line's secondary measurements (taken after the headline figures): an exception is reported in
+    the line as {"error": ...}, with its traceback on stderr, instead of ending the run."""
+    try:
+        return fn(*args)
+    except Exception as exc:   # noqa: BLE001 - any failure of a secondary leg is reported, not raised
+        import traceback
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(exc).__name__}: {exc}"[:300]}
 
 
 def learned_correction_accuracy(snapshots, epochs=20, lr=2e-3):
