@@ -43,7 +43,6 @@ constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
 constexpr uint32_t kExBit = 1u << 26;   // with DSF exclusions: flag of an excluded pair in a list entry
 constexpr long long kSpinLimit = 20000000;  // default barrier wait: ~2 s of 100 ns sleeps
 constexpr int kSmallUnit = 4;   // atoms a warp takes at a time in the list build of one-cell-axis replicas
-constexpr int kSkipU = 8;       // grid strides whose replica indices a rebuild phase loads together
 
 struct RepDev {
   int64_t atom0;
@@ -119,6 +118,7 @@ struct Eng {
   int32_t* fcell;                // per rebuild: prefix over replicas of the flagged cells the warp-per-cell
                                  // list build covers (R + 1 entries), then that build's cell counter
   int32_t* fsmall;               // the same for the atoms of flagged one-cell-axis replicas, then a unit counter
+  int32_t* ftile;                // per rebuild: the flagged replicas' 32-slot tiles (any order), then their count
   const int32_t* ex_start;       // DSF exclusions by atom index within a replica (CSR), or none
   const int32_t* ex_ids;
   int32_t n_ex_ids;
@@ -824,25 +824,23 @@ struct PairScan {
   }
 };
 
-// Grid-stride walk over the slots of flagged replicas (padding slots excluded), calling f(s, r). The replica
-// indices of kSkipU strides are loaded together, so skipping the slots of unflagged replicas costs one memory
-// round trip per kSkipU strides instead of one per stride (an ensemble rebuild touches a few % of its slots).
-template <class FL, class F>
-__device__ __forceinline__ void for_flagged_slots(const Eng& E, const FL& fl, int64_t gtid, int64_t gstride, F&& f) {
-  for (int64_t s0 = gtid; s0 < E.S; s0 += kSkipU * gstride) {
-    unsigned m = 0u;
-#pragma unroll
-    for (int u = 0; u < kSkipU; ++u) {
-      const int64_t s = s0 + u * gstride;
-      if (s < E.S && fl[__ldg(E.tile_rep + (s >> 5))]) m |= 1u << u;
-    }
-    while (m) {
-      const int u = __ffs(m) - 1;
-      m &= m - 1u;
-      const int64_t s = s0 + u * gstride;
-      const int r = __ldg(E.tile_rep + (s >> 5));
-      if (s - E.rep[r].atom0 < E.rep[r].n) f(s, r);
-    }
+// Grid-stride walk over the slots of the rebuild's flagged tiles (listed in phase P0 of this launch, read through
+// L2; padding slots excluded), calling f(s, r); with one replica, which is flagged whenever a rebuild runs, over
+// all its slots. An ensemble rebuild touches a few % of its slots, which this
+// visits without scanning the others; the phases that use it do not depend on the order of the slots.
+template <class F>
+__device__ __forceinline__ void for_flagged_slots(const Eng& E, int64_t gtid, int64_t gstride, F&& f) {
+  if (E.R == 1) {   // one replica, rebuilt: every slot
+    for (int64_t s = gtid; s < E.S; s += gstride)
+      if (s < E.rep[0].n) f(s, 0);
+    return;
+  }
+  const int64_t nslots = (int64_t)__ldcg(E.ftile + (E.S >> 5)) * 32;
+  for (int64_t q = gtid; q < nslots; q += gstride) {
+    const int t = __ldcg(E.ftile + (q >> 5));
+    const int64_t s = (int64_t)t * 32 + (q & 31);
+    const int r = __ldg(E.tile_rep + t);
+    if (s - E.rep[r].atom0 < E.rep[r].n) f(s, r);
   }
 }
 
@@ -969,6 +967,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
       E.fcell[E.R + 1] = 0;   // the list build's cell counter
       E.fsmall[E.R] = total_s;
       E.fsmall[E.R + 1] = 0;  // and its atom-unit counter
+      E.ftile[E.S >> 5] = 0;  // the flagged-tile count
     }
   }
 #define PHASE(k)                                                  \
@@ -980,17 +979,31 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(1);
 
-  // P0: clear counters of flagged replicas' cells
+  // P0: clear counters of flagged replicas' cells; list the flagged replicas' tiles (a warp appends its tiles
+  // with one atomic), which the slot phases then walk instead of skipping the unflagged replicas' slots
   for (int64_t c = gtid; c < E.C; c += gstride) {
     if (fl[E.cell_rep[c]]) {
       E.count[c] = 0;
       E.cursor[c] = 0;
     }
   }
+  if (E.R > 1) {
+    const int lane = threadIdx.x & 31;
+    const int64_t T = E.S >> 5;
+    for (int64_t t0 = gtid - lane; t0 < T; t0 += gstride) {   // gstride is a multiple of 32: warp-uniform
+      const int64_t t = t0 + lane;
+      const bool f = t < T && fl[__ldg(E.tile_rep + t)];
+      const unsigned bal = __ballot_sync(0xffffffffu, f);
+      int base = 0;
+      if (lane == 0 && bal) base = atomicAdd(E.ftile + T, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (f) E.ftile[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)t;
+    }
+  }
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(2);
   // P1: absolute wrapped positions and new cells
-  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t s, int r) {
+  for_flagged_slots(E, gtid, gstride, [&](int64_t s, int r) {
     const RepDev& R = E.rep[r];
     int c0, c1, c2;
     cell_coords(E.cellid[s] - R.cellbase, R, c0, c1, c2);
@@ -1070,14 +1083,14 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(6);
   // P3: scatter old slots to new slots
-  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t s, int) {
+  for_flagged_slots(E, gtid, gstride, [&](int64_t s, int) {
     const int c = E.newcell[s];
     E.perm[E.start[E.crank[c]] + atomicAdd(&E.cursor[c], 1)] = (int32_t)s;
   });
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(7);
   // P3b: deterministic order inside each cell: every atom's rank among its cell's atoms by old slot
-  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int) {
+  for_flagged_slots(E, gtid, gstride, [&](int64_t k, int) {
     const int v = E.perm[k];
     const int c = E.newcell[v];
     const int a0 = E.start[E.crank[c]], a1 = E.start[E.crank[c] + 1];
@@ -1088,7 +1101,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(8);
   // P4: gather into new order
-  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int) {
+  for_flagged_slots(E, gtid, gstride, [&](int64_t k, int) {
     const int o = E.perm2[k];
     E.tmp_cell[k] = E.newcell[o];
     E.tmp_id[k] = E.id[o];
@@ -1102,7 +1115,7 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
   if (!grid_sync(E.bar, E.status, E.spin_limit)) return;
   PHASE(9);
   // P5: commit; offsets from the new cell origins; images
-  for_flagged_slots(E, fl, gtid, gstride, [&](int64_t k, int r) {
+  for_flagged_slots(E, gtid, gstride, [&](int64_t k, int r) {
     const RepDev& R = E.rep[r];
     const int c = E.tmp_cell[k];
     int c0, c1, c2;
@@ -1838,6 +1851,7 @@ Layout make_layout(int32_t R, int64_t S, int32_t T, int32_t C, int32_t NCH, int3
   L.add(4 * (size_t)C);                      // 50 crank (cell id -> slot-order position)
   L.add(4 * (size_t)C);                      // 51 cell_at (position -> cell id)
   L.add(4 * ((size_t)R + 2));                // 52 flagged one-cell-axis atoms prefix, list-build unit counter
+  L.add(4 * ((size_t)T + 1));                // 53 flagged tiles of a rebuild and their count
   return L;
 }
 
@@ -2122,6 +2136,7 @@ int acs_engine_create(const acs_engine_config* cfg, void* mem, size_t bytes, acs
   E.crank = (int32_t*)(b + L.off[50]);
   E.cell_at = (int32_t*)(b + L.off[51]);
   E.fsmall = (int32_t*)(b + L.off[52]);
+  E.ftile = (int32_t*)(b + L.off[53]);
   E.ex_bit = cfg->n_ex_ids > 0 ? kExBit : 0u;
   E.jmask = cfg->n_ex_ids > 0 ? kExBit - 1u : kIdxMask;
   E.thermo = cfg->thermo.kind;
