@@ -269,6 +269,8 @@ def main():
                          "melt, ~45 s); 0 skips it")
     ap.add_argument("--cell-order", type=int, default=1, choices=[0, 1],
                     help="slot order of the cells: 1 Morton (default), 0 row-major")
+    ap.add_argument("--cell-scale", type=float, default=1.0,
+                    help="cell edge of the list build in list radii (1..8; default 1, the narrowest complete stencil)")
     ap.add_argument("--tpa", default=None, help="threads per atom in the pair kernel: 1..32, 'auto' (timed "
                     "autotuner), default: size heuristic")
     ap.add_argument("--experiment", choices=["learned", "drift", "dropin", "correction_kernels", "autotune"],
@@ -324,7 +326,8 @@ def main():
         shard = shard_replicas([x.n for x in systems], world)[rank]
         systems, dts = [systems[r] for r in shard], [dts[r] for r in shard]
     rec_cap = max(args.steps // args.record_every + 2, args.drift_steps // args.record_every + 2, 4)
-    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=rec_cap, tpa=args.tpa, cell_order=args.cell_order)
+    eng, rlist, hs = start_engine(systems, forces, dts, rec_cap=rec_cap, tpa=args.tpa, cell_order=args.cell_order,
+                                  cell_scale=args.cell_scale)
     n = sum(x.n for x in systems)
     pairs_lj, pairs_dsf = eng.count_pairs()
     step_blocks, coop_blocks, slots = eng.launch_info()
@@ -338,7 +341,8 @@ def main():
         eng.check("profile")
         nreb = eng.status().rebuilds - rb0
         ph = {k: round(v / max(nreb, 1), 4) for k, v in eng.phase_times().items()}
-        print(json.dumps({"profile": cfg["workload"], "tpa": eng.tpa, "step_kernel_ms": k_ms, "list_kernel_ms": r_ms,
+        print(json.dumps({"profile": cfg["workload"], "tpa": eng.tpa, "cell_scale": eng.cell_scale,
+                          "step_kernel_ms": k_ms, "list_kernel_ms": r_ms,
                           "rebuilds": nreb, "ms_per_rebuild_by_phase": ph, "pairs_lj": pairs_lj,
                           "pairs_dsf": pairs_dsf, "maxnb": eng.maxnb, "neighbors": eng.neighbor_stats()}))
         return
@@ -835,7 +839,8 @@ def run_experiment(args):
         print(json.dumps(out), flush=True)
     elif args.experiment == "autotune":
         # the tuned launch shape against the size rule on the ensemble's replica sizes: per bucket, 8 replicas of
-        # one fcc size at dt*, every candidate (threads per atom x step grid) timed with per-kernel events
+        # one fcc size at dt*, every candidate (threads per atom x step grid) timed with per-kernel events, then the
+        # wider cell edges for the fastest pair and for the size rule
         from devinproj_b200 import autotune, configs
         from devinproj_b200.engine import default_tpa, estimate_maxnb, forcefield_from, start_engine
         rows = []
@@ -850,19 +855,32 @@ def run_experiment(args):
             vol = sum(float(np.prod(x.box)) for x in systems)
             nb = n_total / vol * 4.0 / 3.0 * math.pi * rlist ** 3
             times = {}
-            for tpa, gm in autotune.candidates(n_total, nb):
-                eng, _, _ = start_engine([x.copy() for x in systems], [lj], dts, tpa=tpa, grid_mult=gm)
+
+            def timed(tpa, gm, cs):
+                eng, _, _ = start_engine([x.copy() for x in systems], [lj], dts, tpa=tpa, grid_mult=gm, cell_scale=cs)
                 eng.run(10, 0, True)
                 k_ms, r_ms, tot = eng.run_timed(max(args.steps, 50), 0)
                 eng.check("autotune experiment")
-                times[f"{tpa},{gm}"] = tot / max(args.steps, 50)
+                times[autotune._label(tpa, gm, cs)] = tot / max(args.steps, 50)
                 del eng
+
+            for tpa, gm in autotune.candidates(n_total, nb):
+                timed(tpa, gm, 1.0)
             cells = sum(int(np.prod([max(1, int(bx // rlist)) for bx in x.box])) for x in systems)
             rule = default_tpa(n_total, (estimate_maxnb(systems[0].n, systems[0].box, rlist) - 32) / 1.3, cells)
+            narrow = {k: v for k, v in times.items() if k.endswith(",1")}
+            pair = min(narrow, key=narrow.get).rsplit(",", 1)[0]
+            for cs in autotune.CELL_SCALES[1:]:   # the tuner's second stage, and the same edges at the size rule
+                timed(*(int(x) for x in pair.split(",")), cs)
+                if f"{rule},0" != pair:
+                    timed(rule, 0, cs)
+            rule_key = autotune._label(rule, 0, 1.0)
             best = min(times, key=times.get)
-            rows.append({"atoms_per_replica": systems[0].n, "replicas": len(systems), "rule": f"{rule},0",
-                         "rule_ms": times.get(f"{rule},0"), "best": best, "best_ms": times[best],
-                         "gain": (times.get(f"{rule},0") or float("nan")) / times[best], "ms_per_step": times})
+            rows.append({"atoms_per_replica": systems[0].n, "replicas": len(systems), "rule": rule_key,
+                         "rule_ms": times.get(rule_key), "best": best, "best_ms": times[best],
+                         "gain": (times.get(rule_key) or float("nan")) / times[best],
+                         "cells_per_axis": {f"{c:g}": int(systems[0].box[0] // (rlist * c)) for c in autotune.CELL_SCALES},
+                         "ms_per_step": times})
             print(json.dumps(rows[-1]), flush=True)
         print(json.dumps({"experiment": "autotune_vs_size_rule", "rows": len(rows)}), flush=True)
     elif args.experiment == "dropin":

@@ -1,11 +1,15 @@
 """Launch-shape autotuner for the engine: threads per atom in the pair kernel (1..32, which also fixes the
-neighbour-list layout) and the step kernel's grid: one thread per slot (`grid_mult` 0), or k blocks per SM that
-loop over the slots (`grid_mult` 4 or 8), which trades the last wave's tail for a loop.
+neighbour-list layout), the step kernel's grid (one thread per slot, `grid_mult` 0, or k blocks per SM that
+loop over the slots, `grid_mult` 4 or 8, which trades the last wave's tail for a loop), and the list build's
+cell edge (`cell_scale` x the list radius: wider cells give a warp more home atoms per cell and more candidates
+per stencil; on small boxes they leave axes with fewer than three cells, which the list build then walks a warp
+per atom).
 
 `tune()` builds the engine for each candidate on the caller's own replicas, times a short eager run with
 CUDA events around every kernel (`acs_engine_run_timed`), and keeps the fastest step + list-maintenance
-time. Results are cached per workload signature (atom count and replica count buckets, list radius and
-density) in a JSON file ($ACS_AUTOTUNE_CACHE, default ~/.cache/accusim_b200/autotune.json).
+time: first every (threads per atom, step grid) pair at the narrowest cells, then the wider cell edges for the
+best pair. Results are cached per workload signature (atom count and replica count buckets, list density, force
+terms, GPU model) in a JSON file ($ACS_AUTOTUNE_CACHE, default ~/.cache/accusim_b200/autotune.json).
 """
 from __future__ import annotations
 
@@ -71,6 +75,9 @@ def _store(db):
         pass
 
 
+CELL_SCALES = (1.0, 1.25, 1.5)   # cell edge / list radius, searched after the (threads per atom, grid) pair
+
+
 def candidates(n_total, nb):
     tpas = [t for t in (1, 2, 4, 8, 16, 32) if t * 2 <= max(nb, 2)]   # at least two list entries per lane
     if n_total > 2_000_000:
@@ -79,31 +86,49 @@ def candidates(n_total, nb):
     return [(t, g) for t in tpas for g in grids]
 
 
+def _label(tpa, gm, cs):
+    return f"{tpa},{gm},{cs:g}"
+
+
+def _best(entry):
+    """(tpa, grid_mult, cell_scale) of a cache entry (entries without a cell edge were tuned at 1)."""
+    b = entry["best"]
+    return int(b[0]), int(b[1]), float(b[2]) if len(b) > 2 else 1.0
+
+
 def tune(systems, forces, dts, steps=30, use_cache=True, verbose=False):
-    """Best (tpa, grid_mult) for these replicas. Runs the engine a few steps per candidate on the GPU."""
+    """Best (tpa, grid_mult, cell_scale) for these replicas. Runs the engine a few steps per candidate on the
+    GPU."""
     from .engine import forcefield_from, start_engine
     _, rlist, _ = forcefield_from(forces, systems[0].species)
     key = signature(systems, rlist, forces)
     db = _load() if use_cache else {}
     if key in db:
-        return tuple(db[key]["best"])
+        return _best(db[key])
     n_total = sum(s.n for s in systems)
     vol = sum(float(np.prod(s.box)) for s in systems)
     nb = n_total / vol * 4.0 / 3.0 * math.pi * rlist ** 3
     results = {}
-    for tpa, gm in candidates(n_total, nb):
-        eng, _, _ = start_engine([s.copy() for s in systems], forces, dts, tpa=tpa, grid_mult=gm)
+
+    def measure(tpa, gm, cs):
+        eng, _, _ = start_engine([s.copy() for s in systems], forces, dts, tpa=tpa, grid_mult=gm, cell_scale=cs)
         eng.run(5, 0, True)
         k_ms, r_ms, tot = eng.run_timed(steps, 0)
         eng.check("autotune")
-        results[f"{tpa},{gm}"] = tot / steps
+        results[_label(tpa, gm, cs)] = tot / steps
         if verbose:
-            print(f"autotune {key}: tpa={tpa} grid_mult={gm}: {tot / steps:.4f} ms/step "
+            print(f"autotune {key}: tpa={tpa} grid_mult={gm} cell_scale={cs:g}: {tot / steps:.4f} ms/step "
                   f"(pair {k_ms:.4f}, list {r_ms:.4f})")
         del eng
+        return tot / steps
+
+    shapes = {(tpa, gm): measure(tpa, gm, CELL_SCALES[0]) for tpa, gm in candidates(n_total, nb)}
+    tpa, gm = min(shapes, key=shapes.get)
+    for cs in CELL_SCALES[1:]:
+        measure(tpa, gm, cs)
     best = min(results, key=results.get)
-    tpa, gm = (int(x) for x in best.split(","))
-    db[key] = {"best": [tpa, gm], "ms_per_step": results}
+    t, g, c = best.split(",")
+    db[key] = {"best": [int(t), int(g), float(c)], "ms_per_step": results}
     if use_cache:
         _store(db)
-    return tpa, gm
+    return int(t), int(g), float(c)

@@ -1696,6 +1696,11 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
     err = ACS_ERR_ARG;
     return;
   }
+  if (!(cfg->cell_scale == 0.0 || (cfg->cell_scale >= 1.0 && cfg->cell_scale <= 8.0))) {
+    err = ACS_ERR_ARG;
+    return;
+  }
+  const double cell_scale = cfg->cell_scale == 0.0 ? 1.0 : cfg->cell_scale;
   if (cfg->thermo.kind < 0 || cfg->thermo.kind > 2 ||
       (cfg->thermo.kind == 1 && !(cfg->thermo.kT >= 0.0 && cfg->thermo.friction >= 0.0)) ||
       (cfg->thermo.kind == 2 && !(cfg->thermo.kT > 0.0 && cfg->thermo.period > 0.0))) {
@@ -1727,8 +1732,9 @@ void plan(const acs_engine_config* cfg, std::vector<RepDev>& reps, std::vector<i
         err = ACS_ERR_ARG;
         return;
       }
-      // cells no narrower than the list radius (so the 27-cell stencil is complete), at most 1024 per edge
-      double f = floor(q.box[d] / q.rlist);
+      // cells no narrower than cell_scale x the list radius (so the 27-cell stencil is complete), at most
+      // 1024 per edge
+      double f = floor(q.box[d] / (q.rlist * cell_scale));
       int nc = f < 1.0 ? 1 : (int)std::min(f, 1024.0);
       while (nc > 1 && q.box[d] / nc < q.rlist) --nc;
       if (nc < 3) nc = 1;

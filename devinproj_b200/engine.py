@@ -56,7 +56,8 @@ class EngineConfig(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("maxnb", C.c_int32), ("rec_cap", C.c_int32), ("grid_mult", C.c_int32),
                 ("tpa", C.c_int32), ("cell_order", C.c_int32), ("replicas", C.POINTER(Replica)), ("ff", ForceField),
                 ("thermo", Thermostat), ("ex_start", C.POINTER(C.c_int32)), ("ex_ids", C.POINTER(C.c_int32)),
-                ("n_ex_ids", C.c_int32), ("pad2", C.c_int32), ("barrier_wait_limit", C.c_int64)]
+                ("n_ex_ids", C.c_int32), ("pad2", C.c_int32), ("barrier_wait_limit", C.c_int64),
+                ("cell_scale", C.c_double)]
 
 
 def langevin_thermostat(integrator, seed):
@@ -158,7 +159,8 @@ class Engine:
     """ctypes wrapper around one acs_engine; device memory is one torch allocation."""
 
     def __init__(self, replicas, ff: ForceField, maxnb: int, rec_cap: int = 64, grid_mult: int = 0, tpa: int = 1,
-                 thermo=None, exclusions=None, barrier_wait_limit: int = 0, cell_order: int = 1):
+                 thermo=None, exclusions=None, barrier_wait_limit: int = 0, cell_order: int = 1,
+                 cell_scale: float = 1.0):
         require_cuda()
         L = _lib.lib()
         for name, (res, args) in ENGINE_SIGNATURES.items():
@@ -180,6 +182,8 @@ class Engine:
         self.cfg.barrier_wait_limit = int(barrier_wait_limit)
         self.cfg.cell_order = int(cell_order)
         self.cell_order = int(cell_order)
+        self.cfg.cell_scale = float(cell_scale)
+        self.cell_scale = float(cell_scale)
         self._ex = exclusions   # (ex_start, ex_ids) int32 arrays, kept alive with the config
         if exclusions is not None:
             ex_start, ex_ids = exclusions
@@ -404,7 +408,7 @@ def dsf_exclusions(forces, systems):
 
 
 def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None,
-                 exclusions=None, barrier_wait_limit=0, cell_order=1):
+                 exclusions=None, barrier_wait_limit=0, cell_order=1, cell_scale=1.0):
     """Create an engine for replicas given in SI [{n, box, dt}], sharing `forces`. Returns
     (engine, rlist, half_skin) with the radii in SI."""
     ff, rlist, half_skin = forcefield_from(forces, species)
@@ -417,7 +421,8 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
         cells = sum(int(np.prod([max(1, int(bx // r["rlist"])) for bx in r["box"]])) for r in reps)
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3, cells)
     return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
-                   exclusions=exclusions, barrier_wait_limit=barrier_wait_limit, cell_order=cell_order), rlist,
+                   exclusions=exclusions, barrier_wait_limit=barrier_wait_limit, cell_order=cell_order,
+                   cell_scale=cell_scale), rlist,
             half_skin)
 
 
@@ -434,7 +439,8 @@ def _upload_state(engine, systems):
     engine.set_state(to_dev(pos), to_dev(vel), to_dev(sp))
 
 
-def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None, cell_order=1):
+def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=None, thermo=None, cell_order=1,
+                 cell_scale=1.0):
     """Engine over the given periodic 3-D systems (one replica each) with state loaded and lists built;
     grows the neighbour capacity once if the first build overflows."""
     for s in systems:
@@ -443,12 +449,13 @@ def start_engine(systems, forces, dts, maxnb=None, rec_cap=64, grid_mult=0, tpa=
     species = systems[0].species
     if tpa == "auto":
         from .autotune import tune
-        tpa, grid_mult = tune(systems, forces, dts)
+        tpa, grid_mult, cell_scale = tune(systems, forces, dts)
     reps = [dict(n=s.n, box=s.box, dt=dt) for s, dt in zip(systems, dts)]
     ex = dsf_exclusions(forces, systems)
     for attempt in range(3):
         eng, rlist, hs = build_engine(reps, forces, species, maxnb=maxnb, rec_cap=rec_cap, grid_mult=grid_mult,
-                                      tpa=tpa, thermo=thermo, exclusions=ex, cell_order=cell_order)
+                                      tpa=tpa, thermo=thermo, exclusions=ex, cell_order=cell_order,
+                                      cell_scale=cell_scale)
         _upload_state(eng, systems)
         st = eng.status()
         if st.flags & _lib.FLAG_OVERFLOW:

@@ -83,6 +83,11 @@ typedef struct acs_engine_config {
    * 0: the default, 2e7 polls (~2 s); negative: no polling (a block that is not the last to arrive gives up
    * at once, which makes the timeout path testable). */
   int64_t barrier_wait_limit;
+  /* Cell edge of the list build, in units of the list radius: cells no narrower than cell_scale x rlist
+   * (0: 1, the narrowest cells the 27-cell stencil covers; otherwise 1 <= cell_scale <= 8). Wider cells put
+   * more home atoms in each cell a warp takes and more candidates in its stencil, and change the slot order;
+   * the neighbour pair set is the same for every value (it is the FP64 filter's at the list radius). */
+  double cell_scale;
 } acs_engine_config;
 
 typedef struct acs_engine acs_engine;

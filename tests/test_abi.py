@@ -109,6 +109,16 @@ def test_engine_config_validation_is_host_side():
     for th in good:
         c4, k4 = _engine_config(thermo=th)
         assert L.acs_engine_bytes(C.byref(c4)) >= ok
+    # the list build's cell edge: 0 (one list radius) or 1..8 list radii; wider cells need fewer cell slots
+    for cs, valid in ((0.0, True), (1.0, True), (1.5, True), (8.0, True), (0.99, False), (0.5, False),
+                      (8.5, False), (float("nan"), False), (-1.0, False)):
+        c5, k5 = _engine_config()
+        c5.cell_scale = cs
+        assert (L.acs_engine_bytes(C.byref(c5)) > 0) == valid, cs
+    c5, k5 = _engine_config(box_sigma=40.0)
+    c6, k6 = _engine_config(box_sigma=40.0)
+    c6.cell_scale = 1.5
+    assert 0 < L.acs_engine_bytes(C.byref(c6)) < L.acs_engine_bytes(C.byref(c5))   # 9^3 cells instead of 14^3
 
 
 def test_engine_dsf_exclusion_tables():

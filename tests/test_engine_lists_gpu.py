@@ -240,3 +240,44 @@ def test_engine_lists_with_a_one_cell_axis(tpa):
             ref = pair_keys(*port.cell_list_pairs(st, rlist), s.n)
             assert compare_sets(got, ref, p, s.box, rlist, f"replica {r} tpa {tpa} block {block}") == 0
     assert eng.status().rebuilds - rb0 >= 4
+
+
+@pytest.mark.parametrize("cell_scale", [1.25, 1.5])
+@pytest.mark.parametrize("tpa", [1, 32])
+def test_engine_lists_with_wider_cells(golden, tpa, cell_scale):
+    """Cells wider than the list radius (the autotuner's cell-edge candidates) change only which candidates a warp
+    screens: on the golden argon system (whose 3 cells per axis then collapse to one, so every axis wraps) the lists
+    hold the reference's pair set, and on a hot 4000-atom fluid (5 cells per axis at edge 1, 4 or 3 when wider) they
+    hold the oracle's pair set on the positions of the last rebuild, at the start and after rebuilds inside graph
+    runs; the final forces match the FP64 oracle."""
+    from devinproj_b200 import LennardJones, configs
+    from devinproj_b200.engine import ACC, LEN, start_engine
+    g = golden("argon864")
+    s = _system(g)
+    lj = LennardJones({"Ar": (float(g["eps"]), float(g["sig"]))}, cutoff=2.5)
+    eng, rlist, _ = start_engine([s], [lj], [float(g["dt"])], tpa=tpa, cell_scale=cell_scale)
+    got, _, pos = engine_pairs(eng)
+    ref = pair_keys(g["pair_i"], g["pair_j"], s.n)
+    assert compare_sets(got, ref, pos, s.box, rlist, f"argon864 cells x{cell_scale} tpa {tpa}") == 0
+    h, lj = configs.lj_fluid(10, seed=5)
+    h.maxwell_boltzmann(300.0, np.random.default_rng(5))
+    eng, rlist, _ = start_engine([h], [lj], [1e-14], tpa=tpa, cell_scale=cell_scale)
+    assert 3 <= int(h.box[0] // (rlist * cell_scale)) < int(h.box[0] // rlist) == 5
+    rb0 = eng.status().rebuilds
+    for block in range(3):
+        if block:
+            eng.run(31, 0, True)
+            eng.check("run")
+        got, _, pos = engine_pairs(eng)
+        st = port.State(pos, np.zeros_like(pos), h.sp.copy(), h.ids.copy(), h.box.copy(), True,
+                        [("Ar", configs.AR_MASS, 0.0)])
+        ref = pair_keys(*port.cell_list_pairs(st, rlist), h.n)
+        assert compare_sets(got, ref, pos, h.box, rlist, f"4000-atom cells x{cell_scale} tpa {tpa} block {block}") == 0
+    assert eng.status().rebuilds - rb0 >= 4
+    p, v, a = eng.get_state()
+    st = port.State(p.cpu().numpy() * LEN, np.zeros((h.n, 3)), h.sp.copy(), h.ids.copy(), h.box.copy(), True,
+                    [("Ar", configs.AR_MASS, 0.0)])
+    Fo, _ = port.LennardJones({"Ar": (configs.AR_EPS, configs.AR_SIGMA)}, cutoff=2.5, skin=0.0).compute(st)
+    F = a.cpu().numpy() * ACC * configs.AR_MASS
+    assert float(np.sqrt(np.mean(np.sum((F - Fo) ** 2, 1)) / np.mean(np.sum(Fo ** 2, 1)))) <= 1e-5
+
