@@ -101,3 +101,58 @@ def test_minimize_follows_the_reference_forces():
         assert np.max(np.abs(d)) <= 1e-9 * s.box[0], kind
         assert np.all(s.vel == 0.0)
         assert np.allclose(sim.force, sim_ref.force, rtol=0, atol=1e-8 * np.max(np.abs(sim_ref.force))), kind
+
+
+def _salt_model(field):
+    """A 512-ion rock-salt model in accusim's JSON form (8^3 sites at 2.82 A, each ion displaced by a seeded 0.1 A
+    so that the forces are not the lattice's zero, velocities at 1100 K): LJ (Lorentz-Berthelot) + DSF at 8 A,
+    Nose-Hoover; with `field`, also a uniform electric field (a force without a GPU plug-in, which stays
+    accusim's)."""
+    n = np.stack(np.meshgrid(*[np.arange(8)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    odd = n.sum(1) % 2 == 1
+    g = (n + 0.5) * 2.82e-10 + np.random.default_rng(7).normal(0.0, 0.1e-10, n.shape)
+    forces = [{"type": "LennardJones", "params": {"Na": ["0.544 kJ/mol", "2.35 A"], "Cl": ["0.418 kJ/mol", "4.40 A"]},
+               "cutoff": 2.5},
+              {"type": "DampedShiftedCoulomb", "rcut": "8 A"}]
+    if field:
+        forces.append({"type": "UniformField", "E": [2e8, 0.0, -1e8]})
+    return {"dim": 3, "box": "22.56 A", "periodic": True, "seed": 4, "temperature": "1100 K",
+            "species": {"Na": {"mass": "22.99 u", "charge": "1 e"}, "Cl": {"mass": "35.45 u", "charge": "-1 e"}},
+            "particles": [{"species": "Na", "pos": g[~odd].tolist()}, {"species": "Cl", "pos": g[odd].tolist()}],
+            "forces": forces, "integrator": {"type": "NoseHoover", "temperature": "1100 K", "period": "0.1 ps"},
+            "dt": "1 fs"}
+
+
+@pytest.mark.parametrize("field", [False, True])
+@pytest.mark.parametrize("resident", [True, False])
+def test_model_built_simulation_moved_to_gpu(field, resident):
+    """accusim.model.build makes the simulation from a JSON model; to_gpu swaps its LJ, DSF and Nose-Hoover for the
+    GPU plug-ins (the field, without a plug-in, stays accusim's and runs through the host protocol). 30 steps then
+    follow the same model run with the reference's own classes: energies, thermostat state and positions within
+    1e-9, and accusim's report still finds the DSF force and the extended-energy row."""
+    import copy
+
+    import accusim
+    from accusim.model import build
+
+    import devinproj_b200 as b200
+    model = _salt_model(field)
+    ref, _ = build(copy.deepcopy(model))
+    sim, _ = build(copy.deepcopy(model))
+    b200.to_gpu(sim, resident=resident)
+    assert type(sim.forces[0]) is b200.LennardJones and type(sim.forces[1]) is b200.DampedShiftedCoulomb
+    assert type(sim.integrator) is b200.NoseHoover
+    assert isinstance(sim.system, b200.GpuSystem) == resident
+    if field:
+        assert type(sim.forces[2]) is accusim.forces.UniformField
+    assert np.allclose(sim.force, ref.force, rtol=0, atol=1e-10 * np.max(np.abs(ref.force)))
+    tr_r = ref.run(steps=30, record_every=5, positions=False)
+    tr = sim.run(steps=30, record_every=5, positions=False)
+    E_r, E = np.asarray(tr_r.total_energy), np.asarray(tr.total_energy)
+    assert np.max(np.abs(E - E_r)) <= 1e-9 * np.max(np.abs(E_r))
+    assert sim.integrator.xi == pytest.approx(ref.integrator.xi, rel=1e-9, abs=1e-9 * abs(ref.integrator.xi) + 1e-30)
+    d = sim.system.pos - ref.system.pos
+    d -= ref.system.box * np.round(d / ref.system.box)
+    assert np.max(np.abs(d)) <= 1e-9 * ref.system.box[0]
+    names = {c.name for c in accusim.AccuracyReport.build(sim).checks}
+    assert "extended energy" in names and "DSF vs Ewald" in names
