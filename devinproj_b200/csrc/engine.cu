@@ -1167,7 +1167,8 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
     // shared memory): for home atom h, two ballots over the batch give its masks (accepted / inside the
     // upper band edge), which lane h keeps. The next raw chunk is loaded while a batch is screened; only the
     // FP64 band decision branches.
-    __shared__ float4 hpos[8][32];
+    // home atoms' negated coordinates, one array per axis: two adjacent home atoms load as one packed FP32 pair
+    __shared__ __align__(8) float hnx[8][32], hny[8][32], hnz[8][32];
     __shared__ float4 bufp[8][64];
     __shared__ uint32_t bufk[8][64];
     __shared__ int selfpos[8][32];
@@ -1250,7 +1251,12 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
         const int64_t i = h0 + hb + (own ? lane : 0);
         const uint32_t hlo = (uint32_t)(h0 + hb);
         __syncwarp();
-        hpos[wib][lane] = im[i];
+        {
+          const float4 hp = im[i];
+          hnx[wib][lane] = -hp.x;
+          hny[wib][lane] = -hp.y;
+          hnz[wib][lane] = -hp.z;
+        }
         int32_t* __restrict__ lst = E.nbr + (i / E.G) * (int64_t)E.maxnb * E.G + (i % E.G);
         int cnt = 0, nbuf = 0, rb = 0;
         float4 rp;
@@ -1284,15 +1290,24 @@ __global__ void __launch_bounds__(256, 3) k_rebuild(Eng E, int dst, int rec, int
           const uint32_t hs = (ck & kIdxMask) - hlo;   // home index of this candidate, if it is a home atom
           if (lane < nk && hs < (uint32_t)nh) selfpos[wib][hs] = lane;
           uint32_t m_in = 0u, m_hi = 0u;
-#pragma unroll 4
-          for (int h = 0; h < nh; ++h) {
-            const float4 hp = hpos[wib][h];
-            const float x = cur.x - hp.x, y = cur.y - hp.y, z = cur.z - hp.z;
-            const float q = x * x + y * y + z * z;
-            const unsigned bi = __ballot_sync(0xffffffffu, q <= lo_f), bh = __ballot_sync(0xffffffffu, q < hi_f);
+          // two home atoms per packed FP32 operation (each half is the IEEE scalar operation); with an odd count
+          // the last pair's second atom is a staged non-home slot, whose masks are cleared below
+          const float2 px = make_float2(cur.x, cur.x), py = make_float2(cur.y, cur.y), pz = make_float2(cur.z, cur.z);
+#pragma unroll 2
+          for (int h = 0; h < nh; h += 2) {
+            const float2 x = __fadd2_rn(px, *reinterpret_cast<const float2*>(&hnx[wib][h]));
+            const float2 y = __fadd2_rn(py, *reinterpret_cast<const float2*>(&hny[wib][h]));
+            const float2 z = __fadd2_rn(pz, *reinterpret_cast<const float2*>(&hnz[wib][h]));
+            const float2 q = __ffma2_rn(z, z, __ffma2_rn(y, y, __fmul2_rn(x, x)));
+            const unsigned bi0 = __ballot_sync(0xffffffffu, q.x <= lo_f), bh0 = __ballot_sync(0xffffffffu, q.x < hi_f);
+            const unsigned bi1 = __ballot_sync(0xffffffffu, q.y <= lo_f), bh1 = __ballot_sync(0xffffffffu, q.y < hi_f);
             if (lane == h) {
-              m_in = bi;
-              m_hi = bh;
+              m_in = bi0;
+              m_hi = bh0;
+            }
+            if (lane == h + 1) {
+              m_in = bi1;
+              m_hi = bh1;
             }
           }
           __syncwarp();
