@@ -418,7 +418,7 @@ def build_engine(replicas_si, forces, species, maxnb=None, rec_cap=64, grid_mult
     if maxnb is None:
         maxnb = expect
     if tpa is None:
-        cells = sum(int(np.prod([max(1, int(bx // r["rlist"])) for bx in r["box"]])) for r in reps)
+        cells = sum(int(np.prod([max(1, int(bx // (r["rlist"] * cell_scale))) for bx in r["box"]])) for r in reps)
         tpa = default_tpa(sum(r["n"] for r in reps), (expect - 32) / 1.3, cells)
     return (Engine(reps, ff, maxnb, rec_cap=rec_cap, grid_mult=grid_mult, tpa=tpa, thermo=thermo,
                    exclusions=exclusions, barrier_wait_limit=barrier_wait_limit, cell_order=cell_order,
