@@ -5,9 +5,11 @@ same systems:
   `Force.compute` twice, so a plug-in that kept a neighbour list or cell grid across the box change would give a
   wrong dU/dV;
 * `minimize` (accusim/minimize.py:11-47, FIRE) calls `Simulation.potential` every step after moving the host
-  positions in place, and finishes with `update_forces`.
+  positions in place, and finishes with `update_forces`;
+* `model.build` (accusim/model.py:102-135) makes a simulation from a JSON model with accusim's own classes, which
+  `to_gpu` moves onto the plug-ins.
 
-Both run on accusim's plain `System` and on the device-resident `GpuSystem`. Tolerances: the FP64 plug-ins' forces
+Each runs on accusim's plain `System` and on the device-resident `GpuSystem`. Tolerances: the FP64 plug-ins' forces
 and energies differ from NumPy's at round-off (tests/test_dropin_gpu.py), which dU/dV's central difference with
 h = 1e-6 lifts to about 1e-9 relative; FIRE's trajectory is damped, so 150 steps keep the positions within 1e-9 of
 the box edge of the reference's."""
