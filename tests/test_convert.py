@@ -47,3 +47,37 @@ def test_others_come_back_unchanged():
     keep.append(MyLJ({"Ar": (1.6e-21, 3.4e-10)}))
     for obj in keep:
         assert b200.gpu_twin(obj) is obj
+
+
+def test_to_gpu_decides_where_the_state_lives(monkeypatch):
+    """to_gpu swaps forces and integrator always, and the system for a GpuSystem only when asked, for 3-D systems
+    and simulations without reactions (accusim's reaction engine keeps the system it was built with); it then
+    recomputes the forces once (a stand-in here: no GPU)."""
+    from devinproj_b200 import configs, convert
+    from devinproj_b200 import state as st
+
+    made = []
+    monkeypatch.setattr(st.GpuSystem, "from_system", classmethod(lambda cls, s: made.append(s) or ("gpu", s)))
+
+    class FakeSim:
+        def __init__(self, system, reactions=None):
+            self.system, self.reactions = system, reactions
+            self.forces = [accusim.forces.LennardJones({"Ar": (1.6e-21, 3.4e-10)}),
+                           accusim.forces.UniformField(E=[1.0, 0.0, 0.0])]
+            self.integrator = accusim.integrators.VelocityVerlet()
+            self.updates = 0
+
+        def update_forces(self):
+            self.updates += 1
+
+    s, _ = configs.lj_fluid(2, seed=0)
+    sim = convert.to_gpu(FakeSim(s))
+    assert sim.system == ("gpu", s) and made == [s] and sim.updates == 1
+    assert type(sim.forces[0]) is b200.LennardJones and type(sim.forces[1]) is accusim.forces.UniformField
+    assert type(sim.integrator) is b200.VelocityVerlet
+    for kw, sim in (({"resident": False}, FakeSim(s)), ({}, FakeSim(s, reactions=object()))):
+        convert.to_gpu(sim, **kw)
+        assert sim.system is s and type(sim.forces[0]) is b200.LennardJones and sim.updates == 1
+    flat = accusim.System(2, box=[1e-9, 1e-9], periodic=True)
+    sim = convert.to_gpu(FakeSim(flat))
+    assert sim.system is flat and made == [s]
